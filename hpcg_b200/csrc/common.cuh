@@ -1,0 +1,113 @@
+// common.cuh -- shared types and device helpers of libhpcgx.
+//
+// Device layout of one multigrid level ("colour-sorted sliced ELL"):
+//   * rows are stored colour-major: colour c = (ix&1) + 2(iy&1) + 4(iz&1), the
+//     8-colouring that the reference's greedy multicolouring produces on the
+//     27-point stencil (src/OptimizeProblem.cpp:43-96); inside a colour, rows
+//     keep natural order, so each colour is a list of x-lines (fixed iy, iz)
+//     holding every other point;
+//   * every colour starts on a 32-row boundary; rows are grouped in slices of
+//     32 and a slice stores its 27 slots column-major: element (row k, slot s)
+//     lives at (k/32)*27*32 + s*32 + k%32, so a warp reading one slot of 32
+//     consecutive rows issues one 256-byte (FP64) load;
+//   * slot s is the stencil offset (dz+1)*9 + (dy+1)*3 + (dx+1); slot 13 is the
+//     diagonal.  Absent neighbours (boundary rows) hold value 0 and column =
+//     the row itself.  Present entries therefore appear in exactly the
+//     (sz, sy, sx) order the reference generator emits
+//     (src/GenerateProblem_ref.cpp:152-172), which makes every row sum below
+//     round exactly as the reference's;
+//   * columns are int32 natural row indices; vectors stay in natural order.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#define HPCGX_STENCIL 27
+#define HPCGX_SLICE 32
+#define HPCGX_DIAG_SLOT 13
+
+namespace hpcgx {
+
+// Largest number of multigrid levels (the reference fixes 4, src/main.cpp:139).
+constexpr int kMaxLevels = 4;
+
+// The four x-line classes of a level: class q = (iy&1) + 2(iz&1).  Class q
+// holds colours 2q (even ix) and 2q+1 (odd ix).
+struct ClassInfo {
+  int q, py, pz;
+  int nyq;          // lines of this class along y
+  int lines;        // lines of this class
+  int len[2];       // rows per line for px = 0 / 1
+  int64_t start[2]; // storage row of the first row of colour 2q+px
+};
+
+// What a kernel needs to know about one level's matrix.
+template <class VT>
+struct LevelMat {
+  const VT *vals;
+  const int32_t *cols;
+  int nx, ny, nz;
+  int64_t n;
+};
+
+__host__ __device__ inline int64_t ell_index(int64_t k, int s) {
+  return (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (int64_t)s * HPCGX_SLICE + (k & 31);
+}
+
+// Colour of the neighbour in slot s of a row of colour c.
+__host__ __device__ constexpr int slot_mask(int s) {
+  return ((s % 3) != 1 ? 1 : 0) | (((s / 3) % 3) != 1 ? 2 : 0) | ((s / 9) != 1 ? 4 : 0);
+}
+
+// Arithmetic with one rounding per operation and no contraction into FMA,
+// so that device sums reproduce the reference's x86-64 rounding bit for bit.
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_div(float a, float b) { return __fdiv_rn(a, b); }
+
+// Matrix value -> arithmetic type.
+__device__ __forceinline__ double to_arith(double v, double) { return v; }
+__device__ __forceinline__ float to_arith(uint16_t h, float) {
+  return __uint_as_float(((uint32_t)h) << 16);
+}
+// Vector value -> arithmetic type (the finest level of the mixed V-cycle
+// reads its FP64 right-hand side and rounds it to FP32 where it is read).
+__device__ __forceinline__ double vec_to(double v, double) { return v; }
+__device__ __forceinline__ float vec_to(double v, float) { return __double2float_rn(v); }
+__device__ __forceinline__ float vec_to(float v, float) { return v; }
+
+// FP64 -> BF16 exactly as the oracle does: round to FP32, then round the FP32
+// bit pattern to BF16 (nearest-even); NaN stays a quiet NaN.
+__host__ __device__ inline uint16_t bf16_from_double(double v) {
+  float f = (float)v;
+  uint32_t u;
+#ifdef __CUDA_ARCH__
+  u = __float_as_uint(f);
+#else
+  __builtin_memcpy(&u, &f, 4);
+#endif
+  if ((u & 0x7f800000u) == 0x7f800000u && (u & 0x007fffffu)) return (uint16_t)((u >> 16) | 0x40);
+  uint32_t lsb = (u >> 16) & 1u;
+  u += 0x7fffu + lsb;
+  return (uint16_t)(u >> 16);
+}
+
+// SplitMix64 (Steele, Lea, Flood 2014) and the counter-based draws built on
+// it; the oracle implements the same functions on the host.
+__host__ __device__ inline uint64_t splitmix64(uint64_t x) {
+  uint64_t z = x + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__host__ __device__ inline double uniform01(uint64_t seed, uint64_t i) {
+  uint64_t h = splitmix64(splitmix64(seed) + i);
+  return (double)(h >> 11) * 0x1.0p-53;
+}
+
+}  // namespace hpcgx

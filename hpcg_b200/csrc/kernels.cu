@@ -1,0 +1,1005 @@
+// kernels.cu -- the sm_100a kernels of libhpcgx.
+//
+// All kernels are HBM-bandwidth bound (no step of HPCG's PCG iteration is a
+// dense contraction, so nothing here uses tensor cores).  The design points:
+//   * stencil rows are walked by x-line classes (fixed iy&1, iz&1): a CTA owns
+//     whole x-lines and treats the even-x rows, then the odd-x rows of those
+//     lines, so the vector sectors a line touches are completed by one CTA
+//     while they sit in L2;
+//   * a Gauss-Seidel half sweep is ONE launch per class: the two colours of a
+//     class only depend on each other along x inside a line, so a
+//     __syncthreads between them replaces a second launch (8 launches per
+//     symmetric sweep instead of 16);
+//   * restriction (src/ComputeRestriction_ref.cpp:51) is fused into the last
+//     colour of the pre-smoother's backward sweep and prolongation
+//     (src/ComputeProlongation_ref.cpp:49) into the first colour of the
+//     post-smoother's forward sweep: the injected points are exactly colour 0;
+//   * the first forward sweep of ComputeMG starts from x = 0
+//     (src/ComputeMG_ref.cpp:42) and skips every term that multiplies a zero;
+//   * reductions are deterministic: fixed per-block partials, then the last
+//     block to finish sums them in index order and applies the CG scalar
+//     update, so alpha/beta never leave the device.
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace hpcgx {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+// ---------------------------------------------------------------- reductions
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <bool MAX>
+__device__ __forceinline__ double warp_red(double v) {
+  return MAX ? warp_max(v) : warp_sum(v);
+}
+
+// Reduces NV values over the block and publishes one partial per block; the
+// last block to arrive sums all partials in block order and returns true with
+// the totals in tot (valid in every thread of that block).  Deterministic for
+// a fixed grid size.
+template <int NV, bool MAX = false>
+__device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&tot)[NV]) {
+  __shared__ double sh[NV][32];
+  __shared__ double fin[NV];
+  __shared__ int amlast;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double t = warp_red<MAX>(v[i]);
+    if (lane == 0) sh[i][wid] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double t = MAX ? 0.0 : 0.0;
+      for (int w = 0; w < nw; ++w) t = MAX ? fmax(t, sh[i][w]) : t + sh[i][w];
+      red.partials[(int64_t)i * gridDim.x + blockIdx.x] = t;
+    }
+    __threadfence();
+    unsigned int prev = atomicAdd(red.counter, 1u);
+    amlast = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!amlast) return false;
+  __threadfence();
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double t = 0.0;
+    for (int64_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+      double p = __ldcg(red.partials + (int64_t)i * gridDim.x + b);
+      t = MAX ? fmax(t, p) : t + p;
+    }
+    t = warp_red<MAX>(t);
+    __syncthreads();
+    if (lane == 0) sh[i][wid] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s = MAX ? fmax(s, sh[i][w]) : s + sh[i][w];
+      fin[i] = s;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NV; ++i) tot[i] = fin[i];
+  if (threadIdx.x == 0) *red.counter = 0u;
+  return true;
+}
+
+// The scalar step that follows a reduction (done by one thread of the last
+// block).  The formulas are CG's (src/CG.cpp:93-124).
+template <int NV>
+__device__ void finish(int fin, void *target, const double (&tot)[NV]) {
+  if (fin == FIN_STORE || fin == FIN_MAX) {
+    double *o = static_cast<double *>(target);
+    for (int i = 0; i < NV; ++i) o[i] = tot[i];
+    return;
+  }
+  CgState *st = static_cast<CgState *>(target);
+  switch (fin) {
+    case FIN_CG_INIT:
+      st->normr = sqrt(tot[0]);
+      st->normr0 = st->normr;
+      st->k = 1;
+      st->niters = 0;
+      st->nonfinite = !isfinite(st->normr);
+      st->done = !(st->normr / st->normr0 > st->tol) || st->max_iter < 1 || st->nonfinite;
+      break;
+    case FIN_CG_RZ:
+      if (st->k == 1) {
+        st->rtz = tot[0];
+      } else {
+        st->oldrtz = st->rtz;
+        st->rtz = tot[0];
+        if (st->flexible) {
+          st->zAp = tot[NV > 1 ? 1 : 0];
+          st->beta = -st->zAp / st->pAp;
+        } else {
+          st->beta = st->rtz / st->oldrtz;
+        }
+      }
+      break;
+    case FIN_CG_PAP:
+      st->pAp = tot[0];
+      st->alpha = st->rtz / st->pAp;
+      break;
+    case FIN_CG_RR:
+      st->normr = sqrt(tot[0]);
+      st->niters = st->k;
+      st->k += 1;
+      st->nonfinite = !isfinite(st->normr);
+      st->done = !(st->normr / st->normr0 > st->tol) || st->k > st->max_iter || st->nonfinite;
+      break;
+    default:
+      break;
+  }
+}
+
+// ---------------------------------------------------------------- geometry
+
+struct ClassSet {
+  ClassInfo c[4];
+  int lpb[4];      // lines per block
+  int first[5];    // first block of each class (prefix sums)
+};
+
+// Row handled by thread-slot t of half px in a block that owns lines [j0, ...).
+struct RowId {
+  int64_t row;   // natural index
+  int64_t k;     // storage row
+  int ix, iy, iz;
+};
+
+__device__ __forceinline__ RowId row_of(const ClassInfo &C, int nx, int ny, int px, int j0,
+                                        int t) {
+  const int Lp = C.len[px];
+  const int jl = t / Lp;
+  const int pos = t - jl * Lp;
+  const int j = j0 + jl;
+  RowId r;
+  r.iy = C.py + 2 * (j % C.nyq);
+  r.iz = C.pz + 2 * (j / C.nyq);
+  r.ix = px + 2 * pos;
+  r.row = ((int64_t)r.iz * ny + r.iy) * nx + r.ix;
+  r.k = C.start[px] + (int64_t)j * Lp + pos;
+  return r;
+}
+
+// ---------------------------------------------------------------- SpMV
+
+// y = A x, rows summed left to right over the slots as ComputeSPMV_ref does
+// (src/ComputeSPMV_ref.cpp:64-70).  With DOT, also reduces sum_i x_i y_i (the
+// p.Ap of CG, src/CG.cpp:119) and runs the finishing scalar step.
+template <class VT, class T, bool DOT>
+__global__ void __launch_bounds__(kThreads)
+k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, Reduce red,
+       int fin, void *fin_target, const int *__restrict__ done) {
+  if (done && *done) return;
+  int q = 0;
+#pragma unroll
+  for (int i = 1; i < 4; ++i)
+    if ((int)blockIdx.x >= cs.first[i]) q = i;
+  const ClassInfo &C = cs.c[q];
+  const int j0 = ((int)blockIdx.x - cs.first[q]) * cs.lpb[q];
+  const int j1 = min(j0 + cs.lpb[q], C.lines);
+  double acc = 0.0;
+  for (int px = 0; px < 2; ++px) {
+    const int cnt = (j1 - j0) * C.len[px];
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
+      const int64_t base = (id.k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (id.k & 31);
+      T sum = T(0);
+      T xrow = T(0);
+#pragma unroll
+      for (int s = 0; s < HPCGX_STENCIL; ++s) {
+        const T v = to_arith(__ldg(A.vals + base + s * HPCGX_SLICE), T());
+        const T xv = __ldg(x + __ldg(A.cols + base + s * HPCGX_SLICE));
+        if (s == HPCGX_DIAG_SLOT) xrow = xv;
+        sum = rn_add(sum, rn_mul(v, xv));
+      }
+      y[id.row] = sum;
+      if (DOT) acc += (double)xrow * (double)sum;
+    }
+  }
+  if (DOT) {
+    double v[1] = {acc}, tot[1];
+    if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(fin, fin_target, tot);
+  }
+}
+
+// ---------------------------------------------------------------- Gauss-Seidel
+
+// One Gauss-Seidel row update, src/ComputeSYMGS_ref.cpp:72-80:
+//   sum = r_i - sum_j a_ij x_j (diagonal included, slot order); sum += x_i a_ii;
+//   x_i = sum / a_ii.
+// ZERO: x is known to be zero for every colour above c and for row i itself
+//       (first forward sweep after ZeroVector); those terms are skipped, which
+//       changes nothing but possibly the sign of an exact zero.
+// PRO:  x_i first receives the prolongated coarse correction (colour 0).
+// RES:  after the update, the fine residual at this injected point is formed
+//       and restricted: rc = r_i - (A x)_i with (A x)_i summed as in SpMV.
+template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
+__device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, int c,
+                                       const RT *__restrict__ r, T *x, const T *__restrict__ xc,
+                                       T *__restrict__ rc) {
+  const int64_t base = (id.k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (id.k & 31);
+  const T rhs = vec_to(__ldg(r + id.row), T());
+  int64_t crow = 0;
+  if (PRO || RES) {
+    const int nxc = A.nx >> 1, nyc = A.ny >> 1;
+    crow = ((int64_t)(id.iz >> 1) * nyc + (id.iy >> 1)) * nxc + (id.ix >> 1);
+  }
+  T xi = ZERO ? T(0) : x[id.row];
+  if (PRO) xi = rn_add(xi, __ldg(xc + crow));
+  T sum = rhs;
+  T d = T(1);
+#pragma unroll
+  for (int s = 0; s < HPCGX_STENCIL; ++s) {
+    const T v = to_arith(__ldg(A.vals + base + s * HPCGX_SLICE), T());
+    if (s == HPCGX_DIAG_SLOT) {
+      d = v;
+      if (!ZERO) sum = rn_sub(sum, rn_mul(v, xi));
+      continue;
+    }
+    if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
+    const int32_t col = __ldg(A.cols + base + s * HPCGX_SLICE);
+    sum = rn_sub(sum, rn_mul(v, x[col]));
+  }
+  if (!ZERO) sum = rn_add(sum, rn_mul(xi, d));
+  const T xn = rn_div(sum, d);
+  x[id.row] = xn;
+  if (RES) {
+    T ax = T(0);
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      const T v = to_arith(__ldg(A.vals + base + s * HPCGX_SLICE), T());
+      const T xv = (s == HPCGX_DIAG_SLOT) ? xn : x[__ldg(A.cols + base + s * HPCGX_SLICE)];
+      ax = rn_add(ax, rn_mul(v, xv));
+    }
+    rc[crow] = rn_sub(rhs, ax);
+  }
+}
+
+// A half sweep over one class: colours 2q then 2q+1 (forward) or 2q+1 then 2q
+// (backward).  MODE bits: GS_ZERO_GUESS for the whole launch; GS_PROLONG and
+// GS_RESTRICT act on colour 0 only.
+template <int MODE, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads)
+k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, int backward, const RT *__restrict__ r, T *x,
+           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
+  if (done && *done) return;
+  constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0;
+  constexpr bool PRO = (MODE & GS_PROLONG) != 0;
+  constexpr bool RES = (MODE & GS_RESTRICT) != 0;
+  const int j0 = blockIdx.x * lpb;
+  const int j1 = min(j0 + lpb, C.lines);
+  for (int half = 0; half < 2; ++half) {
+    const int px = backward ? 1 - half : half;
+    const int c = px + 2 * C.q;
+    const int cnt = (j1 - j0) * C.len[px];
+    for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+      const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
+      if ((PRO || RES) && c == 0)
+        gs_row<ZERO, PRO, RES>(A, id, c, r, x, xc, rc);
+      else
+        gs_row<ZERO, false, false>(A, id, c, r, x, xc, rc);
+    }
+    if (half == 0) __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- vectors
+
+__global__ void __launch_bounds__(kThreads)
+k_waxpby(int64_t n, double alpha, const double *__restrict__ x, double beta,
+         const double *__restrict__ y, double *w, const int *__restrict__ done) {
+  if (done && *done) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  // The three branches of src/ComputeWAXPBY_ref.cpp:52-67 round differently.
+  if (alpha == 1.0) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+      w[i] = rn_add(x[i], rn_mul(beta, y[i]));
+  } else if (beta == 1.0) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+      w[i] = rn_add(rn_mul(alpha, x[i]), y[i]);
+  } else {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+      w[i] = rn_add(rn_mul(alpha, x[i]), rn_mul(beta, y[i]));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_dot(int64_t n, const double *__restrict__ x, const double *__restrict__ y, Reduce red,
+      double *out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    acc += x[i] * y[i];
+  double v[1] = {acc}, tot[1];
+  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) out[0] = tot[0];
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_absmax_diff(int64_t n, const double *__restrict__ a, const double *__restrict__ b, Reduce red,
+              double *out) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double m = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
+    m = fmax(m, fabs(a[i] - b[i]));
+  double v[1] = {m}, tot[1];
+  if (grid_reduce<1, true>(v, red, tot) && threadIdx.x == 0) out[0] = tot[0];
+}
+
+__device__ __forceinline__ int64_t fine_of_coarse(int64_t ic, int nxf, int nyf) {
+  const int nxc = nxf >> 1, nyc = nyf >> 1;
+  const int64_t ixc = ic % nxc, iyc = (ic / nxc) % nyc, izc = ic / ((int64_t)nxc * nyc);
+  return (2 * izc) * (int64_t)nxf * nyf + (2 * iyc) * (int64_t)nxf + 2 * ixc;
+}
+
+// src/ComputeRestriction_ref.cpp:51 with f2c of src/GenerateCoarseProblem.cpp:71-82.
+__global__ void k_restriction(int64_t nc, int nxf, int nyf, const double *__restrict__ rf,
+                              const double *__restrict__ Axf, double *rc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t f = fine_of_coarse(i, nxf, nyf);
+    rc[i] = rn_sub(rf[f], Axf[f]);
+  }
+}
+
+// src/ComputeProlongation_ref.cpp:49.
+__global__ void k_prolongation(int64_t nc, int nxf, int nyf, const double *__restrict__ xc,
+                               double *xf) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t f = fine_of_coarse(i, nxf, nyf);
+    xf[f] = rn_add(xf[f], xc[i]);
+  }
+}
+
+__global__ void k_copy(int64_t n, const double *__restrict__ x, double *y,
+                       const int *__restrict__ done) {
+  if (done && *done) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i];
+}
+
+__global__ void k_fill_uniform(int64_t n, uint64_t seed, double lo, double hi, double *v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = rn_add(lo, rn_mul(rn_sub(hi, lo), uniform01(seed, (uint64_t)i)));
+}
+
+__device__ __forceinline__ double normal01(uint64_t seed, uint64_t i) {
+  const double u1 = 1.0 - uniform01(seed, 2 * i);
+  const double u2 = uniform01(seed, 2 * i + 1);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+__global__ void k_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double *v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = normal01(seed, offset + (uint64_t)i);
+}
+
+// ---------------------------------------------------------------- CG pieces
+
+// r = b - Ap (WAXPBY(1, b, -1, Ap), src/CG.cpp:88) and |r|^2 -> normr0.
+__global__ void __launch_bounds__(kThreads)
+k_cg_init(int64_t n, const double *__restrict__ b, const double *__restrict__ Ap, double *r,
+          Reduce red, CgState *st) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double ri = rn_add(b[i], rn_mul(-1.0, Ap[i]));
+    r[i] = ri;
+    acc += ri * ri;
+  }
+  double v[1] = {acc}, tot[1];
+  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(FIN_CG_INIT, st, tot);
+}
+
+// rtz = r.z (src/CG.cpp:109/112); for the flexible solver also z.Ap_{k-1}.
+template <class ZT, bool FLEX>
+__global__ void __launch_bounds__(kThreads)
+k_cg_rz(int64_t n, const double *__restrict__ r, const ZT *__restrict__ z,
+        const double *__restrict__ Ap, Reduce red, CgState *st) {
+  if (st->done) return;
+  const bool two = FLEX && st->k > 1;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double a0 = 0.0, a1 = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double zi = (double)z[i];
+    a0 += r[i] * zi;
+    if (two) a1 += zi * Ap[i];
+  }
+  if (FLEX) {
+    double v[2] = {a0, a1}, tot[2];
+    if (grid_reduce<2>(v, red, tot) && threadIdx.x == 0) finish<2>(FIN_CG_RZ, st, tot);
+  } else {
+    double v[1] = {a0}, tot[1];
+    if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(FIN_CG_RZ, st, tot);
+  }
+}
+
+// p = z (k == 1) or p = z + beta p (WAXPBY(1, z, beta, p), src/CG.cpp:115).
+template <class ZT>
+__global__ void __launch_bounds__(kThreads)
+k_cg_p(int64_t n, const ZT *__restrict__ z, double *p, const CgState *__restrict__ st) {
+  if (st->done) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const bool first = st->k == 1;
+  const double beta = st->beta;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    const double zi = (double)z[i];
+    p[i] = first ? zi : rn_add(zi, rn_mul(beta, p[i]));
+  }
+}
+
+// x += alpha p; r -= alpha Ap; |r|^2 (src/CG.cpp:121-124).
+__global__ void __launch_bounds__(kThreads)
+k_cg_xr(int64_t n, const double *__restrict__ p, const double *__restrict__ Ap, double *x,
+        double *r, Reduce red, CgState *st) {
+  if (st->done) return;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const double alpha = st->alpha, malpha = -st->alpha;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    x[i] = rn_add(x[i], rn_mul(alpha, p[i]));
+    const double ri = rn_add(r[i], rn_mul(malpha, Ap[i]));
+    r[i] = ri;
+    acc += ri * ri;
+  }
+  double v[1] = {acc}, tot[1];
+  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(FIN_CG_RR, st, tot);
+}
+
+__global__ void k_copy_z(int64_t n, const double *__restrict__ r, double *z,
+                         const CgState *__restrict__ st) {
+  if (st->done) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = r[i];
+}
+
+// ---------------------------------------------------------------- set-up
+
+struct Geo {
+  int nx, ny, nz;
+  int64_t cstart[8], ccount[8];
+  int len[2];
+  int nyq[4];
+};
+
+__device__ __forceinline__ bool storage_to_natural(const Geo &g, int64_t k, int64_t &row, int &ix,
+                                                   int &iy, int &iz) {
+  int c = 0;
+#pragma unroll
+  for (int i = 1; i < 8; ++i)
+    if (k >= g.cstart[i]) c = i;
+  const int64_t rem = k - g.cstart[c];
+  if (rem >= g.ccount[c]) return false;
+  const int px = c & 1, q = c >> 1, py = q & 1, pz = q >> 1;
+  const int Lp = g.len[px];
+  const int64_t j = rem / Lp;
+  const int pos = (int)(rem - j * Lp);
+  iy = py + 2 * (int)(j % g.nyq[q]);
+  iz = pz + 2 * (int)(j / g.nyq[q]);
+  ix = px + 2 * pos;
+  row = ((int64_t)iz * g.ny + iy) * g.nx + ix;
+  return true;
+}
+
+__device__ __forceinline__ int64_t natural_to_storage(const Geo &g, int64_t row) {
+  const int ix = (int)(row % g.nx);
+  const int iy = (int)((row / g.nx) % g.ny);
+  const int iz = (int)(row / ((int64_t)g.nx * g.ny));
+  const int px = ix & 1, q = (iy & 1) + 2 * (iz & 1);
+  const int c = px + 2 * q;
+  const int64_t j = (int64_t)(iz >> 1) * g.nyq[q] + (iy >> 1);
+  return g.cstart[c] + j * g.len[px] + (ix >> 1);
+}
+
+__device__ __forceinline__ bool neighbour(const Geo &g, int ix, int iy, int iz, int s,
+                                          int64_t row, int64_t &col) {
+  const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+  const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+  if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) return false;
+  col = row + (int64_t)dz * g.nx * g.ny + (int64_t)dy * g.nx + dx;
+  return true;
+}
+
+// The reference problem (src/GenerateProblem_ref.cpp:152-172) written
+// straight into the device layout: 26 on the diagonal, -1 elsewhere.
+__global__ void k_generate_hpcg(Geo g, int64_t storage_rows, double *vals, int32_t *cols) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < storage_rows;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t row;
+    int ix, iy, iz;
+    const bool real = storage_to_natural(g, k, row, ix, iy, iz);
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      int64_t col = 0;
+      double v = 0.0;
+      if (real) {
+        if (neighbour(g, ix, iy, iz, s, row, col))
+          v = (s == HPCGX_DIAG_SLOT) ? 26.0 : -1.0;
+        else
+          col = row;
+      }
+      vals[base + s * HPCGX_SLICE] = v;
+      cols[base + s * HPCGX_SLICE] = (int32_t)col;
+    }
+  }
+}
+
+// Variable-coefficient SPD matrix (the oracle's or_generate_varcoef): each
+// undirected edge {lo, hi} draws z ~ N(0,1) keyed by the finest-level index of
+// lo and the direction, a = -exp(sigma z); diagonal = sum |a| + 2.
+__global__ void k_generate_varcoef(Geo g, int64_t storage_rows, int level, int nx0, int ny0,
+                                   uint64_t seed, double sigma, double *vals, int32_t *cols) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < storage_rows;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t row;
+    int ix, iy, iz;
+    const bool real = storage_to_natural(g, k, row, ix, iy, iz);
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    double dsum = 0.0;
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      int64_t col = 0;
+      double v = 0.0;
+      if (real) {
+        if (neighbour(g, ix, iy, iz, s, row, col)) {
+          if (s != HPCGX_DIAG_SLOT) {
+            int lx = ix, ly = iy, lz = iz, h = s - 14;
+            if (s < HPCGX_DIAG_SLOT) {
+              lx = ix + (s % 3 - 1);
+              ly = iy + ((s / 3) % 3 - 1);
+              lz = iz + (s / 9 - 1);
+              h = 12 - s;
+            }
+            const int64_t lo = ((int64_t)(lz << level) * ny0 + (ly << level)) * nx0 + (lx << level);
+            v = -exp(sigma * normal01(seed, (uint64_t)lo * 13u + (uint64_t)h));
+            dsum += fabs(v);
+          }
+        } else {
+          col = row;
+        }
+      }
+      vals[base + s * HPCGX_SLICE] = v;
+      cols[base + s * HPCGX_SLICE] = (int32_t)col;
+    }
+    if (real) vals[base + HPCGX_DIAG_SLOT * HPCGX_SLICE] = dsum + 2.0;
+  }
+}
+
+// Coarse variable-coefficient operator from the fine one: the coarse edge
+// {lo, lo+d} takes the fine value of the edge leaving the injected point of lo
+// in direction d; the diagonal is again sum |a| + 2.
+__global__ void k_coarsen_varcoef(Geo gf, Geo gc, int64_t storage_rows_c,
+                                  const double *__restrict__ fvals, double *cvals) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < storage_rows_c;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t row;
+    int ix, iy, iz;
+    if (!storage_to_natural(gc, k, row, ix, iy, iz)) continue;
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    double dsum = 0.0;
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      if (s == HPCGX_DIAG_SLOT) continue;
+      int64_t col;
+      if (!neighbour(gc, ix, iy, iz, s, row, col)) continue;
+      int lx = ix, ly = iy, lz = iz, sl = s;
+      if (s < HPCGX_DIAG_SLOT) {
+        lx = ix + (s % 3 - 1);
+        ly = iy + ((s / 3) % 3 - 1);
+        lz = iz + (s / 9 - 1);
+        sl = 26 - s;
+      }
+      const int64_t frow = ((int64_t)(2 * lz) * gf.ny + 2 * ly) * gf.nx + 2 * lx;
+      const int64_t fk = natural_to_storage(gf, frow);
+      const double v = fvals[(fk >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (int64_t)sl * HPCGX_SLICE +
+                             (fk & 31)];
+      cvals[base + s * HPCGX_SLICE] = v;
+      dsum += fabs(v);
+    }
+    cvals[base + HPCGX_DIAG_SLOT * HPCGX_SLICE] = dsum + 2.0;
+  }
+}
+
+__global__ void k_to_bf16(int64_t m, const double *__restrict__ v, uint16_t *h) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x)
+    h[i] = bf16_from_double(v[i]);
+}
+
+// Values in natural row order, 27 stencil slots per row -> device layout.
+// Slots without a neighbour stay 0 whatever the input holds.
+__global__ void k_set_values(Geo g, int64_t n, const double *__restrict__ in, double *vals) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = natural_to_storage(g, row);
+    const int ix = (int)(row % g.nx), iy = (int)((row / g.nx) % g.ny),
+              iz = (int)(row / ((int64_t)g.nx * g.ny));
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      int64_t col;
+      const bool has = neighbour(g, ix, iy, iz, s, row, col);
+      vals[base + s * HPCGX_SLICE] = has ? in[row * HPCGX_STENCIL + s] : 0.0;
+    }
+  }
+}
+
+__global__ void k_get_values(Geo g, int64_t n, const double *__restrict__ vals,
+                             const int32_t *__restrict__ cols, double *out, int32_t *cout) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = natural_to_storage(g, row);
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      if (out) out[row * HPCGX_STENCIL + s] = vals[base + s * HPCGX_SLICE];
+      if (cout) cout[row * HPCGX_STENCIL + s] = cols[base + s * HPCGX_SLICE];
+    }
+  }
+}
+
+__global__ void k_set_diagonal(Geo g, int64_t n, const double *__restrict__ d, double *vals) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = natural_to_storage(g, row);
+    vals[(k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + HPCGX_DIAG_SLOT * HPCGX_SLICE + (k & 31)] = d[row];
+  }
+}
+
+__global__ void k_get_diagonal(Geo g, int64_t n, const double *__restrict__ vals, double *d) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = natural_to_storage(g, row);
+    d[row] = vals[(k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + HPCGX_DIAG_SLOT * HPCGX_SLICE + (k & 31)];
+  }
+}
+
+// dL/da_ij = -lambda_i x_j for every stored slot, natural row order, 27 slots
+// per row (zero where the stencil has no neighbour).
+__global__ void k_adjoint_grad(Geo g, int64_t n, const int32_t *__restrict__ cols,
+                               const double *__restrict__ lambda, const double *__restrict__ x,
+                               double *grad) {
+  for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = natural_to_storage(g, row);
+    const int ix = (int)(row % g.nx), iy = (int)((row / g.nx) % g.ny),
+              iz = (int)(row / ((int64_t)g.nx * g.ny));
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    const double li = lambda[row];
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      int64_t col;
+      const bool has = neighbour(g, ix, iy, iz, s, row, col);
+      grad[row * HPCGX_STENCIL + s] =
+          has ? -(li * x[__ldg(cols + base + s * HPCGX_SLICE)]) : 0.0;
+    }
+  }
+}
+
+Geo geo_of(const LevelDev &L) {
+  Geo g;
+  g.nx = L.nx;
+  g.ny = L.ny;
+  g.nz = L.nz;
+  for (int c = 0; c < 8; ++c) {
+    g.cstart[c] = L.cstart[c];
+    g.ccount[c] = L.ccount[c];
+  }
+  g.len[0] = L.cls[0].len[0];
+  g.len[1] = L.cls[0].len[1];
+  for (int q = 0; q < 4; ++q) g.nyq[q] = L.cls[q].nyq;
+  return g;
+}
+
+int grid_for(int64_t n, int threads = kThreads) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 16));
+}
+
+template <class VT>
+LevelMat<VT> mat_of(const LevelDev &L, const VT *vals) {
+  LevelMat<VT> A;
+  A.vals = vals;
+  A.cols = L.cols;
+  A.nx = L.nx;
+  A.ny = L.ny;
+  A.nz = L.nz;
+  A.n = L.n;
+  return A;
+}
+
+ClassSet classes_of(const LevelDev &L) {
+  ClassSet cs;
+  int b = 0;
+  for (int q = 0; q < 4; ++q) {
+    cs.c[q] = L.cls[q];
+    cs.lpb[q] = L.lines_per_block[q];
+    cs.first[q] = b;
+    b += L.blocks[q];
+  }
+  cs.first[4] = b;
+  return cs;
+}
+
+}  // namespace
+
+// ======================================================================== host
+// Every launch_* returns the number of kernels it launched (0 or 1).
+
+int vector_blocks(int64_t n) {
+  int64_t b = (n + kThreads * 4 - 1) / (kThreads * 4);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 8));
+}
+
+void plan_level(LevelDev &L, int nx, int ny, int nz) {
+  L.nx = nx;
+  L.ny = ny;
+  L.nz = nz;
+  L.n = (int64_t)nx * ny * nz;
+  int64_t start = 0;
+  for (int c = 0; c < 8; ++c) {
+    const int px = c & 1, py = (c >> 1) & 1, pz = (c >> 2) & 1;
+    const int64_t cx = (nx - px + 1) / 2, cy = (ny - py + 1) / 2, cz = (nz - pz + 1) / 2;
+    L.ccount[c] = cx * cy * cz;
+    L.cstart[c] = start;
+    start += (L.ccount[c] + 31) / 32 * 32;
+  }
+  L.storage_rows = start;
+  L.spmv_blocks = 0;
+  for (int q = 0; q < 4; ++q) {
+    ClassInfo &C = L.cls[q];
+    C.q = q;
+    C.py = q & 1;
+    C.pz = q >> 1;
+    C.nyq = (ny - C.py + 1) / 2;
+    const int nzq = (nz - C.pz + 1) / 2;
+    C.lines = C.nyq * nzq;
+    C.len[0] = (nx + 1) / 2;
+    C.len[1] = nx / 2;
+    C.start[0] = L.cstart[2 * q];
+    C.start[1] = L.cstart[2 * q + 1];
+    const int len = std::max(C.len[0], 1);
+    int lpb = std::max(1, kThreads / len);
+    lpb = std::min(lpb, std::max(C.lines, 1));
+    L.lines_per_block[q] = lpb;
+    L.blocks[q] = C.lines > 0 ? (C.lines + lpb - 1) / lpb : 0;
+    int th = std::min(kThreads, ((lpb * len) + 31) / 32 * 32);
+    L.threads[q] = std::max(th, 32);
+    L.spmv_blocks += L.blocks[q];
+  }
+}
+
+int64_t storage_row_host(const LevelDev &L, int64_t row) {
+  const int ix = (int)(row % L.nx), iy = (int)((row / L.nx) % L.ny),
+            iz = (int)(row / ((int64_t)L.nx * L.ny));
+  const int px = ix & 1, q = (iy & 1) + 2 * (iz & 1), c = px + 2 * q;
+  const int64_t j = (int64_t)(iz >> 1) * L.cls[q].nyq + (iy >> 1);
+  return L.cstart[c] + j * L.cls[q].len[px] + (ix >> 1);
+}
+
+int launch_generate_hpcg(const LevelDev &L, cudaStream_t s) {
+  k_generate_hpcg<<<grid_for(L.storage_rows), kThreads, 0, s>>>(geo_of(L), L.storage_rows, L.vals,
+                                                                L.cols);
+  return 1;
+}
+
+int launch_generate_varcoef(const LevelDev &L, int level, int nx0, int ny0, uint64_t seed,
+                            double sigma, cudaStream_t s) {
+  k_generate_varcoef<<<grid_for(L.storage_rows), kThreads, 0, s>>>(
+      geo_of(L), L.storage_rows, level, nx0, ny0, seed, sigma, L.vals, L.cols);
+  return 1;
+}
+
+int launch_coarsen_varcoef(const LevelDev &F, const LevelDev &Cc, cudaStream_t s) {
+  k_coarsen_varcoef<<<grid_for(Cc.storage_rows), kThreads, 0, s>>>(geo_of(F), geo_of(Cc),
+                                                                    Cc.storage_rows, F.vals, Cc.vals);
+  return 1;
+}
+
+int launch_to_bf16(const LevelDev &L, cudaStream_t s) {
+  const int64_t m = L.storage_rows * HPCGX_STENCIL;
+  k_to_bf16<<<grid_for(m), kThreads, 0, s>>>(m, L.vals, L.vals16);
+  return 1;
+}
+
+int launch_set_values(const LevelDev &L, const double *vals27, cudaStream_t s) {
+  k_set_values<<<grid_for(L.n), kThreads, 0, s>>>(geo_of(L), L.n, vals27, L.vals);
+  return 1;
+}
+
+int launch_get_values(const LevelDev &L, double *vals27, int32_t *cols27, cudaStream_t s) {
+  k_get_values<<<grid_for(L.n), kThreads, 0, s>>>(geo_of(L), L.n, L.vals, L.cols, vals27, cols27);
+  return 1;
+}
+
+int launch_set_diagonal(const LevelDev &L, const double *diag, cudaStream_t s) {
+  k_set_diagonal<<<grid_for(L.n), kThreads, 0, s>>>(geo_of(L), L.n, diag, L.vals);
+  return 1;
+}
+
+int launch_get_diagonal(const LevelDev &L, double *diag, cudaStream_t s) {
+  k_get_diagonal<<<grid_for(L.n), kThreads, 0, s>>>(geo_of(L), L.n, L.vals, diag);
+  return 1;
+}
+
+int launch_spmv(const LevelDev &L, const double *x, double *y, const Reduce *dot, int fin,
+                void *fin_target, const int *done, cudaStream_t s) {
+  if (L.spmv_blocks == 0) return 0;
+  if (dot)
+    k_spmv<double, double, true><<<L.spmv_blocks, kThreads, 0, s>>>(
+        mat_of(L, L.vals), classes_of(L), x, y, *dot, fin, fin_target, done);
+  else
+    k_spmv<double, double, false><<<L.spmv_blocks, kThreads, 0, s>>>(
+        mat_of(L, L.vals), classes_of(L), x, y, Reduce(), 0, nullptr, done);
+  return 1;
+}
+
+int launch_spmv32(const LevelDev &L, const float *x, float *y, cudaStream_t s) {
+  if (L.spmv_blocks == 0) return 0;
+  k_spmv<uint16_t, float, false><<<L.spmv_blocks, kThreads, 0, s>>>(
+      mat_of(L, L.vals16), classes_of(L), x, y, Reduce(), 0, nullptr, nullptr);
+  return 1;
+}
+
+template <class T>
+struct ValsOf;
+template <>
+struct ValsOf<double> {
+  using VT = double;
+  static const double *get(const LevelDev &L) { return L.vals; }
+};
+template <>
+struct ValsOf<float> {
+  using VT = uint16_t;
+  static const uint16_t *get(const LevelDev &L) { return L.vals16; }
+};
+
+template <class T, class RT>
+int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
+                    const T *xc, T *rc, const int *done, cudaStream_t s) {
+  using VT = typename ValsOf<T>::VT;
+  if (L.blocks[q] == 0) return 0;
+  const LevelMat<VT> A = mat_of(L, ValsOf<T>::get(L));
+  const dim3 g(L.blocks[q]), b(L.threads[q]);
+  const int lpb = L.lines_per_block[q];
+  const ClassInfo &C = L.cls[q];
+  switch (mode) {
+    case GS_PLAIN:
+      k_gs_class<GS_PLAIN><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
+      return 1;
+    case GS_ZERO_GUESS:
+      k_gs_class<GS_ZERO_GUESS><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
+      return 1;
+    case GS_RESTRICT:
+      k_gs_class<GS_RESTRICT><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
+      return 1;
+    case GS_PROLONG:
+      k_gs_class<GS_PROLONG><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
+      return 1;
+    default:
+      return 0;
+  }
+}
+
+template int launch_gs_class<double, double>(const LevelDev &, int, int, int, const double *,
+                                             double *, const double *, double *, const int *,
+                                             cudaStream_t);
+template int launch_gs_class<float, double>(const LevelDev &, int, int, int, const double *,
+                                            float *, const float *, float *, const int *,
+                                            cudaStream_t);
+template int launch_gs_class<float, float>(const LevelDev &, int, int, int, const float *,
+                                           float *, const float *, float *, const int *,
+                                           cudaStream_t);
+
+int launch_waxpby(int64_t n, double alpha, const double *x, double beta, const double *y,
+                  double *w, const int *done, cudaStream_t s) {
+  k_waxpby<<<vector_blocks(n), kThreads, 0, s>>>(n, alpha, x, beta, y, w, done);
+  return 1;
+}
+
+int launch_dot(int64_t n, const double *x, const double *y, const Reduce &red, double *out,
+               cudaStream_t s) {
+  k_dot<<<vector_blocks(n), kThreads, 0, s>>>(n, x, y, red, out);
+  return 1;
+}
+
+int launch_absmax_diff(int64_t n, const double *a, const double *b, const Reduce &red,
+                       double *out, cudaStream_t s) {
+  k_absmax_diff<<<vector_blocks(n), kThreads, 0, s>>>(n, a, b, red, out);
+  return 1;
+}
+
+int launch_restriction(int64_t nc, const LevelDev &F, const double *rf, const double *Axf,
+                       double *rc, cudaStream_t s) {
+  k_restriction<<<grid_for(nc), kThreads, 0, s>>>(nc, F.nx, F.ny, rf, Axf, rc);
+  return 1;
+}
+
+int launch_prolongation(int64_t nc, const LevelDev &F, const double *xc, double *xf,
+                        cudaStream_t s) {
+  k_prolongation<<<grid_for(nc), kThreads, 0, s>>>(nc, F.nx, F.ny, xc, xf);
+  return 1;
+}
+
+int launch_copy(int64_t n, const double *x, double *y, const int *done, cudaStream_t s) {
+  k_copy<<<vector_blocks(n), kThreads, 0, s>>>(n, x, y, done);
+  return 1;
+}
+
+int launch_fill_uniform(int64_t n, uint64_t seed, double lo, double hi, double *v,
+                        cudaStream_t s) {
+  k_fill_uniform<<<grid_for(n), kThreads, 0, s>>>(n, seed, lo, hi, v);
+  return 1;
+}
+
+int launch_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double *v, cudaStream_t s) {
+  k_fill_normal<<<grid_for(n), kThreads, 0, s>>>(n, seed, offset, v);
+  return 1;
+}
+
+int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, const Reduce &red,
+                   CgState *st, cudaStream_t s) {
+  k_cg_init<<<vector_blocks(n), kThreads, 0, s>>>(n, b, Ap, r, red, st);
+  return 1;
+}
+
+template <class ZT>
+int launch_cg_rz(int64_t n, const double *r, const ZT *z, const double *Ap, const Reduce &red,
+                 CgState *st, cudaStream_t s) {
+  if (Ap)
+    k_cg_rz<ZT, true><<<vector_blocks(n), kThreads, 0, s>>>(n, r, z, Ap, red, st);
+  else
+    k_cg_rz<ZT, false><<<vector_blocks(n), kThreads, 0, s>>>(n, r, z, Ap, red, st);
+  return 1;
+}
+template int launch_cg_rz<double>(int64_t, const double *, const double *, const double *,
+                                  const Reduce &, CgState *, cudaStream_t);
+template int launch_cg_rz<float>(int64_t, const double *, const float *, const double *,
+                                 const Reduce &, CgState *, cudaStream_t);
+
+template <class ZT>
+int launch_cg_p(int64_t n, const ZT *z, double *p, CgState *st, cudaStream_t s) {
+  k_cg_p<ZT><<<vector_blocks(n), kThreads, 0, s>>>(n, z, p, st);
+  return 1;
+}
+template int launch_cg_p<double>(int64_t, const double *, double *, CgState *, cudaStream_t);
+template int launch_cg_p<float>(int64_t, const float *, double *, CgState *, cudaStream_t);
+
+int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r,
+                 const Reduce &red, CgState *st, cudaStream_t s) {
+  k_cg_xr<<<vector_blocks(n), kThreads, 0, s>>>(n, p, Ap, x, r, red, st);
+  return 1;
+}
+
+int launch_copy_z(int64_t n, const double *r, double *z, const CgState *st, cudaStream_t s) {
+  k_copy_z<<<vector_blocks(n), kThreads, 0, s>>>(n, r, z, st);
+  return 1;
+}
+
+int launch_adjoint_grad(const LevelDev &L, const double *lambda, const double *x, double *grad,
+                        cudaStream_t s) {
+  k_adjoint_grad<<<grid_for(L.n), kThreads, 0, s>>>(geo_of(L), L.n, L.cols, lambda, x, grad);
+  return 1;
+}
+
+}  // namespace hpcgx

@@ -1,0 +1,885 @@
+// problem.cu -- problem set-up, multigrid / CG drivers and the C ABI of libhpcgx.
+//
+// A problem owns one CUDA stream.  Matrix levels live in the colour-sorted
+// sliced-ELL layout described in common.cuh; CG keeps every scalar on the
+// device and runs each iteration as one CUDA graph (the V-cycle's 56 class
+// launches plus the 4 fused vector/SpMV kernels), so the host only reads the
+// residual norm when it has to test convergence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/hpcgx.h"
+#include "kernels.cuh"
+
+using namespace hpcgx;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(e_ == cudaErrorMemoryAllocation ? HPCGX_ENOMEM : HPCGX_ECUDA,   \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));            \
+  } while (0)
+
+#define TRY(expr)               \
+  do {                          \
+    int rc_ = (expr);           \
+    if (rc_ != HPCGX_OK) return rc_; \
+  } while (0)
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Count of the rows of colour c whose slot s has a neighbour (algorithmic
+// byte model: real nonzeros only).
+int64_t axis_count(int n, int p, int d) {
+  int64_t c = 0;
+  for (int i = p; i < n; i += 2)
+    if (i + d >= 0 && i + d < n) ++c;
+  return c;
+}
+
+// Multigrid work vectors of a level by arithmetic type.
+inline double *lvl_x(LevelDev &A, double *) { return A.x64; }
+inline float *lvl_x(LevelDev &A, float *) { return A.x32; }
+inline double *lvl_r(LevelDev &A, double *) { return A.r64; }
+inline float *lvl_r(LevelDev &A, float *) { return A.r32; }
+
+enum GraphKind { G_FP64_PREC = 0, G_FP64_NOPREC = 1, G_MIXED = 2, G_COUNT = 3 };
+
+struct Probe {
+  cudaEvent_t a, b;
+  double bytes;
+};
+
+}  // namespace
+
+struct hpcgx_problem {
+  int device = 0;
+  int nlev = 0;
+  LevelDev L[kMaxLevels];
+  cudaStream_t stream = nullptr;      // stream in use
+  cudaStream_t own_stream = nullptr;  // stream created with the problem
+  bool loaded[kMaxLevels] = {};
+  bool mixed_ready = false;
+  bool mixed_stale = true;
+  // CG work vectors (finest level)
+  double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
+  float *z32 = nullptr;
+  double *tmp = nullptr;      // staging for host diagonals
+  double *result = nullptr;   // device scalars of standalone reductions
+  CgState *st = nullptr;
+  Reduce red;
+  // graphs of one CG iteration
+  cudaGraphExec_t graph[G_COUNT] = {};
+  int graph_kernels[G_COUNT] = {};
+  int graph_probe[G_COUNT] = {};
+  cudaEvent_t phase[G_COUNT][5] = {};
+  // capture bookkeeping
+  bool capturing = false;
+  int capture_kind = 0;
+  int64_t launches = 0;
+  // probe
+  int probe = HPCGX_PROBE_NONE;
+  std::vector<Probe> probes[G_COUNT];
+  std::vector<Probe> event_pool;  // created outside stream capture
+  size_t pool_next = 0;
+  double probe_ms = 0.0, probe_bytes = 0.0;
+  int64_t probe_launches = 0;
+  size_t bytes = 0;
+
+  ~hpcgx_problem();
+  int alloc(void **ptr, size_t n) {
+    cudaError_t e = cudaMalloc(ptr, n);
+    if (e != cudaSuccess) {
+      *ptr = nullptr;
+      return fail(HPCGX_ENOMEM, "cudaMalloc of " + std::to_string(n) + " bytes failed: " +
+                                    cudaGetErrorString(e));
+    }
+    bytes += n;
+    return HPCGX_OK;
+  }
+  void note(int launched) { launches += launched; }
+
+  // ---- byte model of one class launch (for probes)
+  double gs_bytes(int l, int q, int mode, bool mixed) const {
+    const LevelDev &A = L[l];
+    const double vb = mixed ? 2.0 : 8.0, cb = 4.0, xb = mixed ? 4.0 : 8.0;
+    const double rb = (mixed && l > 0) ? 4.0 : 8.0;
+    double total = 0.0;
+    for (int px = 0; px < 2; ++px) {
+      const int c = px + 2 * q, py = q & 1, pz = q >> 1;
+      int64_t rows = A.ccount[c];
+      double nnzb = 0.0;
+      for (int s = 0; s < HPCGX_STENCIL; ++s) {
+        const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+        const int64_t cnt = axis_count(A.nx, px, dx) * axis_count(A.ny, py, dy) *
+                            axis_count(A.nz, pz, dz);
+        const bool skipped = (mode & GS_ZERO_GUESS) && s != HPCGX_DIAG_SLOT &&
+                             ((c ^ slot_mask(s)) > c);
+        nnzb += (double)cnt * (skipped ? vb : vb + cb);
+      }
+      double vec = rows * (rb + xb + ((mode & GS_ZERO_GUESS) ? 0.0 : xb));
+      if ((mode & GS_RESTRICT) && c == 0) vec += rows * xb;
+      if ((mode & GS_PROLONG) && c == 0) vec += rows * xb;
+      total += nnzb + vec;
+    }
+    return total;
+  }
+
+  // ---- probed launch helpers (events only while capturing a graph)
+  template <class F>
+  int probed(bool match, double bytes_model, F &&launch) {
+    const bool use = capturing && match && probe != HPCGX_PROBE_NONE;
+    if (use) {
+      if (pool_next >= event_pool.size()) return fail(HPCGX_ESTATE, "probe event pool exhausted");
+      Probe pr = event_pool[pool_next++];
+      pr.bytes = bytes_model;
+      CK(cudaEventRecordWithFlags(pr.a, stream, cudaEventRecordExternal));
+      int k = launch();
+      CK(cudaEventRecordWithFlags(pr.b, stream, cudaEventRecordExternal));
+      if (k) probes[capture_kind].push_back(pr);
+      note(k);
+    } else {
+      note(launch());
+    }
+    return HPCGX_OK;
+  }
+
+  // ---- multigrid
+  template <class T, class RT0>
+  int gs_launch(int l, int q, int backward, int mode, const void *r, T *x, const T *xc, T *rc,
+                const int *done) {
+    const bool mixed = std::is_same<T, float>::value;
+    const bool match = (probe == HPCGX_PROBE_GS_FINE && l == 0);
+    return probed(match, match ? gs_bytes(l, q, mode, mixed) : 0.0, [&]() {
+      if (l == 0)
+        return launch_gs_class<T, RT0>(L[l], q, backward, mode, static_cast<const RT0 *>(r), x,
+                                       xc, rc, done, stream);
+      return launch_gs_class<T, T>(L[l], q, backward, mode, static_cast<const T *>(r), x, xc,
+                                   rc, done, stream);
+    });
+  }
+
+  // One V-cycle (src/ComputeMG_ref.cpp:39-63) with all levels fused as
+  // described in kernels.cu.  r0 / x0 are the finest level's vectors.
+  template <class T, class RT0>
+  int vcycle(const RT0 *r0, T *x0, const int *done) {
+    const void *rl[kMaxLevels];
+    T *xl[kMaxLevels];
+    for (int l = 0; l < nlev; ++l) {
+      rl[l] = l == 0 ? static_cast<const void *>(r0) : static_cast<const void *>(lvl_r(L[l], (T *)nullptr));
+      xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
+    }
+    // descend: pre-smooth (zero initial guess) and restrict
+    for (int l = 0; l + 1 < nlev; ++l) {
+      for (int q = 0; q < 4; ++q)
+        TRY((gs_launch<T, RT0>(l, q, 0, GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr, done)));
+      for (int q = 3; q >= 0; --q)
+        TRY((gs_launch<T, RT0>(l, q, 1, q == 0 ? GS_RESTRICT : GS_PLAIN, rl[l], xl[l], nullptr,
+                               lvl_r(L[l + 1], (T *)nullptr), done)));
+    }
+    // coarsest level: one symmetric sweep from zero
+    const int c = nlev - 1;
+    for (int q = 0; q < 4; ++q)
+      TRY((gs_launch<T, RT0>(c, q, 0, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
+    for (int q = 3; q >= 0; --q)
+      TRY((gs_launch<T, RT0>(c, q, 1, GS_PLAIN, rl[c], xl[c], nullptr, nullptr, done)));
+    // ascend: prolongate and post-smooth
+    for (int l = nlev - 2; l >= 0; --l) {
+      for (int q = 0; q < 4; ++q)
+        TRY((gs_launch<T, RT0>(l, q, 0, q == 0 ? GS_PROLONG : GS_PLAIN, rl[l], xl[l],
+                               lvl_x(L[l + 1], (T *)nullptr), nullptr, done)));
+      for (int q = 3; q >= 0; --q)
+        TRY((gs_launch<T, RT0>(l, q, 1, GS_PLAIN, rl[l], xl[l], nullptr, nullptr, done)));
+    }
+    return HPCGX_OK;
+  }
+
+  template <class T, class RT>
+  int symgs(int l, const RT *r, T *x) {
+    for (int q = 0; q < 4; ++q) note(launch_gs_class<T, RT>(L[l], q, 0, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
+    for (int q = 3; q >= 0; --q) note(launch_gs_class<T, RT>(L[l], q, 1, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
+    return HPCGX_OK;
+  }
+
+  int check_ready(bool mixed) {
+    for (int l = 0; l < nlev; ++l)
+      if (!loaded[l]) return fail(HPCGX_ESTATE, "matrix level " + std::to_string(l) + " not loaded");
+    if (mixed && (!mixed_ready || mixed_stale)) {
+      for (int l = 0; l < nlev; ++l) {
+        if (!L[l].vals16) TRY(alloc((void **)&L[l].vals16, L[l].storage_rows * HPCGX_STENCIL * 2));
+        note(launch_to_bf16(L[l], stream));
+      }
+      mixed_ready = true;
+      mixed_stale = false;
+    }
+    return HPCGX_OK;
+  }
+
+  // ---- CG
+  int iteration(int kind) {
+    const int64_t n = L[0].n;
+    const int *done = &st->done;
+    if (kind == G_FP64_NOPREC) {
+      note(launch_copy_z(n, r, z, st, stream));
+    } else if (kind == G_FP64_PREC) {
+      TRY((vcycle<double, double>(r, z, done)));
+    } else {
+      TRY((vcycle<float, double>(r, z32, done)));
+    }
+    if (capturing) CK(cudaEventRecordWithFlags(phase[kind][1], stream, cudaEventRecordExternal));
+    if (kind == G_MIXED) {
+      note(launch_cg_rz<float>(n, r, z32, Ap, red, st, stream));
+      note(launch_cg_p<float>(n, z32, p, st, stream));
+    } else {
+      note(launch_cg_rz<double>(n, r, z, nullptr, red, st, stream));
+      note(launch_cg_p<double>(n, z, p, st, stream));
+    }
+    if (capturing) CK(cudaEventRecordWithFlags(phase[kind][2], stream, cudaEventRecordExternal));
+    const bool match = probe == HPCGX_PROBE_SPMV_FINE;
+    double spmv_bytes = 0.0;
+    if (match) {
+      // 12 B per real nonzero, x and y once, plus the fused p.Ap read of nothing extra
+      int64_t nnz = 0;
+      for (int s = 0; s < HPCGX_STENCIL; ++s) {
+        const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+        int64_t cx = 0, cy = 0, cz = 0;
+        for (int i = 0; i < L[0].nx; ++i) cx += (i + dx >= 0 && i + dx < L[0].nx);
+        for (int i = 0; i < L[0].ny; ++i) cy += (i + dy >= 0 && i + dy < L[0].ny);
+        for (int i = 0; i < L[0].nz; ++i) cz += (i + dz >= 0 && i + dz < L[0].nz);
+        nnz += cx * cy * cz;
+      }
+      spmv_bytes = 12.0 * nnz + 16.0 * n;
+    }
+    TRY(probed(match, spmv_bytes, [&]() {
+      return launch_spmv(L[0], p, Ap, &red, FIN_CG_PAP, st, done, stream);
+    }));
+    if (capturing) CK(cudaEventRecordWithFlags(phase[kind][3], stream, cudaEventRecordExternal));
+    note(launch_cg_xr(n, p, Ap, x, r, red, st, stream));
+    if (capturing) CK(cudaEventRecordWithFlags(phase[kind][4], stream, cudaEventRecordExternal));
+    return HPCGX_OK;
+  }
+
+  int build_graph(int kind) {
+    if (graph[kind] && graph_probe[kind] == probe) return HPCGX_OK;
+    if (graph[kind]) {
+      cudaGraphExecDestroy(graph[kind]);
+      graph[kind] = nullptr;
+      probes[kind].clear();
+    }
+    for (int i = 0; i < 5; ++i)
+      if (!phase[kind][i]) CK(cudaEventCreate(&phase[kind][i]));
+    // every launch a probe can bracket in one iteration: 16 class launches
+    // per level and sweep pair, plus the SpMV
+    const size_t need = 16 * kMaxLevels + 1;
+    if (probe != HPCGX_PROBE_NONE) {
+      // events of earlier graphs may still be referenced: keep them, add new
+      while (event_pool.size() - pool_next < need) {
+        Probe pr;
+        CK(cudaEventCreate(&pr.a));
+        CK(cudaEventCreate(&pr.b));
+        pr.bytes = 0.0;
+        event_pool.push_back(pr);
+      }
+    }
+    cudaGraph_t g = nullptr;
+    const int64_t before = launches;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    capture_kind = kind;
+    cudaEventRecordWithFlags(phase[kind][0], stream, cudaEventRecordExternal);
+    int rc = iteration(kind);
+    capturing = false;
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    graph_kernels[kind] = (int)(launches - before);
+    launches = before;
+    if (rc != HPCGX_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CK(e);
+    e = cudaGraphInstantiate(&graph[kind], g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    graph_probe[kind] = probe;
+    return HPCGX_OK;
+  }
+
+  int read_probes(int kind) {
+    for (auto &pr : probes[kind]) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, pr.a, pr.b));
+      probe_ms += ms;
+      probe_bytes += pr.bytes;
+      probe_launches += 1;
+    }
+    return HPCGX_OK;
+  }
+
+  int cg(int kind, const double *bu, double *xu, int max_iter, double tol, int *niters,
+         double *normr, double *normr0, double *times) {
+    TRY(check_ready(kind == G_MIXED));
+    if (max_iter < 0) return fail(HPCGX_EINVAL, "max_iter < 0");
+    const double t0 = now_s();
+    const int64_t n = L[0].n;
+    CgState h;
+    std::memset(&h, 0, sizeof(h));
+    h.tol = tol;
+    h.max_iter = max_iter;
+    h.flexible = kind == G_MIXED;
+    CK(cudaMemcpyAsync(st, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+    // p = x (CopyVector, src/CG.cpp:86); x lives in the problem's own buffer so
+    // that the iteration graph never changes
+    if (xu != x) CK(cudaMemcpyAsync(x, xu, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaMemcpyAsync(p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    note(launch_spmv(L[0], p, Ap, nullptr, 0, nullptr, nullptr, stream));
+    note(launch_cg_init(n, bu, Ap, r, red, st, stream));
+    TRY(build_graph(kind));
+    const bool per_iter = tol > 0.0 || probe != HPCGX_PROBE_NONE || times != nullptr;
+    double t_mg = 0, t_vec = 0, t_spmv = 0;
+    int launched = 0;
+    while (launched < max_iter) {
+      const int batch = per_iter ? 1 : max_iter - launched;
+      for (int i = 0; i < batch; ++i) {
+        CK(cudaGraphLaunch(graph[kind], stream));
+        launches += graph_kernels[kind];
+      }
+      launched += batch;
+      CK(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      if (per_iter && h.niters == launched) {
+        float a = 0, b2 = 0, c = 0;
+        CK(cudaEventElapsedTime(&a, phase[kind][0], phase[kind][1]));
+        CK(cudaEventElapsedTime(&b2, phase[kind][1], phase[kind][2]));
+        CK(cudaEventElapsedTime(&c, phase[kind][2], phase[kind][3]));
+        float d = 0;
+        CK(cudaEventElapsedTime(&d, phase[kind][3], phase[kind][4]));
+        t_mg += a * 1e-3;
+        t_vec += (b2 + d) * 1e-3;
+        t_spmv += c * 1e-3;
+        TRY(read_probes(kind));
+      }
+      if (h.done) break;
+    }
+    if (xu != x) CK(cudaMemcpyAsync(xu, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (niters) *niters = h.niters;
+    if (normr) *normr = h.normr;
+    if (normr0) *normr0 = h.normr0;
+    if (times) {
+      times[0] += now_s() - t0;
+      times[2] += t_vec;
+      times[3] += t_spmv;
+      times[5] += t_mg;
+    }
+    if (h.nonfinite) return fail(HPCGX_ENONFINITE, "CG: residual norm is not finite");
+    return HPCGX_OK;
+  }
+};
+
+hpcgx_problem::~hpcgx_problem() {
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto &pr : event_pool) {
+    cudaEventDestroy(pr.a);
+    cudaEventDestroy(pr.b);
+  }
+  for (int k = 0; k < G_COUNT; ++k) {
+    if (graph[k]) cudaGraphExecDestroy(graph[k]);
+    for (int i = 0; i < 5; ++i)
+      if (phase[k][i]) cudaEventDestroy(phase[k][i]);
+  }
+  for (int l = 0; l < kMaxLevels; ++l) {
+    cudaFree(L[l].vals);
+    cudaFree(L[l].cols);
+    cudaFree(L[l].vals16);
+    cudaFree(L[l].r64);
+    cudaFree(L[l].x64);
+    cudaFree(L[l].r32);
+    cudaFree(L[l].x32);
+  }
+  for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)z, (void *)p, (void *)Ap,
+                    (void *)z32, (void *)tmp, (void *)result, (void *)st,
+                    (void *)red.partials, (void *)red.counter})
+    cudaFree(ptr);
+  if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+namespace {
+
+#define HANDLE(p)                                                          \
+  do {                                                                     \
+    if (!(p)) return fail(HPCGX_EINVAL, "null problem handle");            \
+    cudaError_t e_ = cudaSetDevice((p)->device);                          \
+    if (e_ != cudaSuccess) return fail(HPCGX_ECUDA, cudaGetErrorString(e_)); \
+  } while (0)
+
+int check_level(hpcgx_problem *p, int level) {
+  if (level < 0 || level >= p->nlev)
+    return fail(HPCGX_EINVAL, "level " + std::to_string(level) + " out of range");
+  return HPCGX_OK;
+}
+
+// Shared body of the two host loaders: get(i, j, col, val) yields entry j of
+// row i.
+template <class Nnz, class Get>
+int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
+  TRY(check_level(p, level));
+  LevelDev &A = p->L[level];
+  const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
+  std::vector<double> vals(slots, 0.0);
+  std::vector<int32_t> cols(slots, 0);
+  for (int64_t row = 0; row < A.n; ++row) {
+    const int ix = (int)(row % A.nx), iy = (int)((row / A.nx) % A.ny),
+              iz = (int)(row / ((int64_t)A.nx * A.ny));
+    const int64_t k = storage_row_host(A, row);
+    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
+    for (int s = 0; s < HPCGX_STENCIL; ++s) cols[base + s * HPCGX_SLICE] = (int32_t)row;
+    const int nz = nnz_of(row);
+    if (nz < 1 || nz > HPCGX_STENCIL)
+      return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + " has " + std::to_string(nz) +
+                                     " entries");
+    int last = -1;
+    bool diag = false;
+    for (int j = 0; j < nz; ++j) {
+      int32_t col;
+      double v;
+      get(row, j, col, v);
+      if (col < 0 || col >= A.n)
+        return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + ": column out of range");
+      const int jx = col % A.nx, jy = (col / A.nx) % A.ny, jz = (int)(col / ((int64_t)A.nx * A.ny));
+      const int dx = jx - ix, dy = jy - iy, dz = jz - iz;
+      if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1)
+        return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + ": column " +
+                                       std::to_string(col) + " is not a stencil neighbour");
+      const int s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+      if (s <= last)
+        return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) +
+                                       ": entries not in stencil order");
+      last = s;
+      diag |= (s == HPCGX_DIAG_SLOT);
+      vals[base + s * HPCGX_SLICE] = v;
+      cols[base + s * HPCGX_SLICE] = col;
+    }
+    if (!diag) return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + " has no diagonal");
+  }
+  CK(cudaMemcpyAsync(A.vals, vals.data(), slots * sizeof(double), cudaMemcpyHostToDevice,
+                     p->stream));
+  CK(cudaMemcpyAsync(A.cols, cols.data(), slots * sizeof(int32_t), cudaMemcpyHostToDevice,
+                     p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  p->loaded[level] = true;
+  p->mixed_stale = true;
+  return HPCGX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *hpcgx_last_error(void) { return g_err.c_str(); }
+
+int hpcgx_version(void) { return 1; }
+
+int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem **out) {
+  if (!out) return fail(HPCGX_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1 || levels < 1 || levels > kMaxLevels)
+    return fail(HPCGX_EINVAL, "bad geometry or level count");
+  if ((int64_t)nx * ny * nz >= (int64_t)1 << 31)
+    return fail(HPCGX_EINVAL, "more than 2^31 rows: column indices are int32");
+  for (int l = 0; l + 1 < levels; ++l)
+    if (((nx >> l) & 1) || ((ny >> l) & 1) || ((nz >> l) & 1))
+      return fail(HPCGX_EINVAL, "level dimensions must be even to coarsen");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(HPCGX_ECUDA, cudaGetErrorString(e));
+  hpcgx_problem *p = new hpcgx_problem;
+  p->device = device;
+  p->nlev = levels;
+  int rc = HPCGX_OK;
+  auto bail = [&](int code) {
+    delete p;
+    return code;
+  };
+  e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(fail(HPCGX_ECUDA, cudaGetErrorString(e)));
+  p->stream = p->own_stream;
+  int64_t red_cap = 0;
+  for (int l = 0; l < levels; ++l) {
+    LevelDev &A = p->L[l];
+    plan_level(A, nx >> l, ny >> l, nz >> l);
+    const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
+    if ((rc = p->alloc((void **)&A.vals, slots * sizeof(double)))) return bail(rc);
+    if ((rc = p->alloc((void **)&A.cols, slots * sizeof(int32_t)))) return bail(rc);
+    if (l > 0) {
+      if ((rc = p->alloc((void **)&A.r64, A.n * sizeof(double)))) return bail(rc);
+      if ((rc = p->alloc((void **)&A.x64, A.n * sizeof(double)))) return bail(rc);
+      if ((rc = p->alloc((void **)&A.r32, A.n * sizeof(float)))) return bail(rc);
+      if ((rc = p->alloc((void **)&A.x32, A.n * sizeof(float)))) return bail(rc);
+    }
+    red_cap = std::max<int64_t>(red_cap, A.spmv_blocks);
+  }
+  const int64_t n = p->L[0].n;
+  red_cap = 2 * std::max<int64_t>(red_cap, vector_blocks(n));
+  for (double **v : {&p->b, &p->x, &p->r, &p->z, &p->p, &p->Ap, &p->tmp})
+    if ((rc = p->alloc((void **)v, n * sizeof(double)))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->z32, n * sizeof(float)))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->result, 4 * sizeof(double)))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->st, sizeof(CgState)))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->red.partials, red_cap * sizeof(double)))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->red.counter, sizeof(unsigned int)))) return bail(rc);
+  p->red.capacity = red_cap;
+  e = cudaMemsetAsync(p->red.counter, 0, sizeof(unsigned int), p->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+  if (e != cudaSuccess) return bail(fail(HPCGX_ECUDA, cudaGetErrorString(e)));
+  *out = p;
+  return HPCGX_OK;
+}
+
+int hpcgx_destroy(hpcgx_problem *p) {
+  if (!p) return HPCGX_OK;
+  delete p;
+  return HPCGX_OK;
+}
+
+int64_t hpcgx_rows(hpcgx_problem *p, int level) {
+  if (!p || level < 0 || level >= p->nlev) return -1;
+  return p->L[level].n;
+}
+
+int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz, const int32_t *cols,
+                     const double *vals) {
+  HANDLE(p);
+  if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
+  return load_level_impl(
+      p, level, [&](int64_t i) { return (int)nnz[i]; },
+      [&](int64_t i, int j, int32_t &c, double &v) {
+        c = cols[i * HPCGX_STENCIL + j];
+        v = vals[i * HPCGX_STENCIL + j];
+      });
+}
+
+int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz,
+                          const int32_t *const *cols, const double *const *vals) {
+  HANDLE(p);
+  if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
+  return load_level_impl(
+      p, level, [&](int64_t i) { return (int)(unsigned char)nnz[i]; },
+      [&](int64_t i, int j, int32_t &c, double &v) {
+        c = cols[i][j];
+        v = vals[i][j];
+      });
+}
+
+int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c, int64_t nc) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (level + 1 >= p->nlev) return fail(HPCGX_EINVAL, "coarsest level has no injection");
+  const LevelDev &F = p->L[level];
+  const int nxc = F.nx / 2, nyc = F.ny / 2, nzc = F.nz / 2;
+  if (nc != (int64_t)nxc * nyc * nzc) return fail(HPCGX_ELAYOUT, "f2c length mismatch");
+  for (int64_t ic = 0; ic < nc; ++ic) {
+    const int64_t ixc = ic % nxc, iyc = (ic / nxc) % nyc, izc = ic / ((int64_t)nxc * nyc);
+    const int64_t f = (2 * izc) * (int64_t)F.nx * F.ny + (2 * iyc) * (int64_t)F.nx + 2 * ixc;
+    if (f2c[ic] != f) return fail(HPCGX_ELAYOUT, "f2c is not the geometric injection");
+  }
+  return HPCGX_OK;
+}
+
+int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma) {
+  HANDLE(p);
+  for (int l = 0; l < p->nlev; ++l) {
+    if (kind == HPCGX_GEN_HPCG) {
+      p->note(launch_generate_hpcg(p->L[l], p->stream));
+    } else if (kind == HPCGX_GEN_VARCOEF) {
+      p->note(launch_generate_varcoef(p->L[l], l, p->L[0].nx, p->L[0].ny, seed, sigma, p->stream));
+    } else {
+      return fail(HPCGX_EINVAL, "unknown generator kind");
+    }
+    p->loaded[l] = true;
+  }
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  p->mixed_stale = true;
+  return HPCGX_OK;
+}
+
+int hpcgx_build_mixed(hpcgx_problem *p) {
+  HANDLE(p);
+  p->mixed_stale = true;
+  TRY(p->check_ready(true));
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+int hpcgx_set_diagonal_host(hpcgx_problem *p, int level, const double *diag) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  const LevelDev &A = p->L[level];
+  CK(cudaMemcpyAsync(p->tmp, diag, A.n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  p->note(launch_set_diagonal(A, p->tmp, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  p->mixed_stale = true;
+  return HPCGX_OK;
+}
+
+int hpcgx_get_diagonal_host(hpcgx_problem *p, int level, double *diag) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  const LevelDev &A = p->L[level];
+  p->note(launch_get_diagonal(A, p->tmp, p->stream));
+  CK(cudaMemcpyAsync(diag, p->tmp, A.n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+int hpcgx_set_values(hpcgx_problem *p, int level, const double *vals27, int recoarsen) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  p->note(launch_set_values(p->L[level], vals27, p->stream));
+  p->loaded[level] = true;
+  if (recoarsen)
+    for (int l = level; l + 1 < p->nlev; ++l) {
+      p->note(launch_coarsen_varcoef(p->L[l], p->L[l + 1], p->stream));
+      p->loaded[l + 1] = true;
+    }
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  p->mixed_stale = true;
+  return HPCGX_OK;
+}
+
+int hpcgx_get_values(hpcgx_problem *p, int level, double *vals27, int32_t *cols27) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  p->note(launch_get_values(p->L[level], vals27, cols27, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+int hpcgx_memory_bytes(hpcgx_problem *p, double *bytes) {
+  if (!p || !bytes) return fail(HPCGX_EINVAL, "null argument");
+  *bytes = (double)p->bytes;
+  return HPCGX_OK;
+}
+
+int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  p->note(launch_spmv(p->L[level], x, y, nullptr, 0, nullptr, nullptr, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  TRY((p->symgs<double, double>(level, r, x)));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
+  HANDLE(p);
+  TRY(p->check_ready(false));
+  TRY((p->vcycle<double, double>(r, x, nullptr)));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  TRY(p->check_ready(true));
+  p->note(launch_spmv32(p->L[level], x, y, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const float *r32,
+                      float *x) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  TRY(p->check_ready(true));
+  if ((r64 == nullptr) == (r32 == nullptr)) return fail(HPCGX_EINVAL, "give exactly one of r64, r32");
+  if (r64)
+    TRY((p->symgs<float, double>(level, r64, x)));
+  else
+    TRY((p->symgs<float, float>(level, r32, x)));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x) {
+  HANDLE(p);
+  TRY(p->check_ready(true));
+  TRY((p->vcycle<float, double>(r, x, nullptr)));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_restriction(hpcgx_problem *p, int level, const double *rf, const double *Axf,
+                      double *rc) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (level + 1 >= p->nlev) return fail(HPCGX_EINVAL, "coarsest level has no restriction");
+  p->note(launch_restriction(p->L[level + 1].n, p->L[level], rf, Axf, rc, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_prolongation(hpcgx_problem *p, int level, const double *xc, double *xf) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (level + 1 >= p->nlev) return fail(HPCGX_EINVAL, "coarsest level has no prolongation");
+  p->note(launch_prolongation(p->L[level + 1].n, p->L[level], xc, xf, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_dot(hpcgx_problem *p, int64_t n, const double *x, const double *y, double *result) {
+  HANDLE(p);
+  if (n < 0 || n > p->L[0].n || !result) return fail(HPCGX_EINVAL, "bad dot arguments");
+  p->note(launch_dot(n, x, y, p->red, p->result, p->stream));
+  CK(cudaMemcpyAsync(result, p->result, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+int hpcgx_waxpby(hpcgx_problem *p, int64_t n, double alpha, const double *x, double beta,
+                 const double *y, double *w) {
+  HANDLE(p);
+  if (n < 0) return fail(HPCGX_EINVAL, "negative length");
+  p->note(launch_waxpby(n, alpha, x, beta, y, w, nullptr, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_residual(hpcgx_problem *p, int64_t n, const double *v1, const double *v2,
+                   double *result) {
+  HANDLE(p);
+  if (n < 0 || n > p->L[0].n || !result) return fail(HPCGX_EINVAL, "bad residual arguments");
+  p->note(launch_absmax_diff(n, v1, v2, p->red, p->result, p->stream));
+  CK(cudaMemcpyAsync(result, p->result, sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
+             int precond, int *niters, double *normr, double *normr0, double *times) {
+  HANDLE(p);
+  return p->cg(precond ? G_FP64_PREC : G_FP64_NOPREC, b, x, max_iter, tolerance, niters, normr,
+               normr0, times);
+}
+
+int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
+                   int *niters, double *normr, double *normr0, double *times) {
+  HANDLE(p);
+  return p->cg(G_MIXED, b, x, max_iter, tolerance, niters, normr, normr0, times);
+}
+
+int hpcgx_cg_host(hpcgx_problem *p, int mixed, const double *b_host, double *x_host, int max_iter,
+                  double tolerance, int *niters, double *normr, double *normr0, double *times) {
+  HANDLE(p);
+  const int64_t n = p->L[0].n;
+  CK(cudaMemcpyAsync(p->b, b_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaMemcpyAsync(p->x, x_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  TRY(p->cg(mixed ? G_MIXED : G_FP64_PREC, p->b, p->x, max_iter, tolerance, niters, normr, normr0,
+            times));
+  CK(cudaMemcpyAsync(x_host, p->x, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, double *grad) {
+  HANDLE(p);
+  p->note(launch_adjoint_grad(p->L[0], lambda, x, grad, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_fill_uniform(hpcgx_problem *p, int64_t n, uint64_t seed, double lo, double hi,
+                       double *v) {
+  HANDLE(p);
+  p->note(launch_fill_uniform(n, seed, lo, hi, v, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_fill_normal(hpcgx_problem *p, int64_t n, uint64_t seed, uint64_t offset, double *v) {
+  HANDLE(p);
+  p->note(launch_fill_normal(n, seed, offset, v, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_set_probe(hpcgx_problem *p, int probe) {
+  HANDLE(p);
+  if (probe < HPCGX_PROBE_NONE || probe > HPCGX_PROBE_SPMV_FINE)
+    return fail(HPCGX_EINVAL, "unknown probe");
+  p->probe = probe;
+  return HPCGX_OK;
+}
+
+int hpcgx_probe_read(hpcgx_problem *p, double *ms, int64_t *launches, double *bytes, int reset) {
+  if (!p) return fail(HPCGX_EINVAL, "null problem handle");
+  if (ms) *ms = p->probe_ms;
+  if (launches) *launches = p->probe_launches;
+  if (bytes) *bytes = p->probe_bytes;
+  if (reset) {
+    p->probe_ms = 0.0;
+    p->probe_bytes = 0.0;
+    p->probe_launches = 0;
+  }
+  return HPCGX_OK;
+}
+
+int64_t hpcgx_launch_count(hpcgx_problem *p) { return p ? p->launches : -1; }
+
+int hpcgx_set_stream(hpcgx_problem *p, void *stream) {
+  HANDLE(p);
+  CK(cudaStreamSynchronize(p->stream));
+  p->stream = stream ? static_cast<cudaStream_t>(stream) : p->own_stream;
+  return HPCGX_OK;
+}
+
+int hpcgx_synchronize(hpcgx_problem *p) {
+  HANDLE(p);
+  CK(cudaStreamSynchronize(p->stream));
+  return HPCGX_OK;
+}
+
+}  // extern "C"

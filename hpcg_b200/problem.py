@@ -1,0 +1,264 @@
+"""Python host API over libhpcgx: HPCG's operators on torch CUDA tensors.
+
+``Problem`` mirrors the reference's replaceable operator set
+(src/ComputeSPMV.hpp, ComputeSYMGS.hpp, ComputeMG.hpp, ComputeDotProduct.hpp,
+ComputeWAXPBY.hpp, ComputeResidual.hpp, CG.hpp, OptimizeProblem.hpp) with the
+same argument meaning and the same 0/non-zero status convention, turned into
+Python exceptions (``HPCGXError``).  Vectors are float64 (float32 for the
+mixed-precision V-cycle) CUDA tensors in natural row order.
+
+All library work runs on one torch stream owned by the problem; every call
+first makes that stream wait for the caller's current stream, and returns
+after the library has synchronised, so results are ready when a method
+returns.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib
+
+STENCIL = 27
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data_as(C.c_void_p)
+    return C.c_void_p(t.data_ptr())
+
+
+class Problem:
+    """One nx*ny*nz HPCG problem with ``levels`` multigrid levels on a GPU."""
+
+    def __init__(self, nx, ny, nz, levels=4, device=0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("hpcg_b200 needs a CUDA device")
+        self.dims = (nx, ny, nz)
+        self.levels = levels
+        self.device = torch.device("cuda", device)
+        h = C.c_void_p()
+        check(lib().hpcgx_create(device, nx, ny, nz, levels, C.byref(h)))
+        self.h = h
+        self.stream = torch.cuda.Stream(device=self.device)
+        check(lib().hpcgx_set_stream(self.h, C.c_void_p(self.stream.cuda_stream)))
+
+    # ----------------------------------------------------------- lifetime
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hpcgx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _pre(self):
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+
+    def rows(self, level=0):
+        return int(lib().hpcgx_rows(self.h, level))
+
+    def level_dims(self, level=0):
+        nx, ny, nz = self.dims
+        return nx >> level, ny >> level, nz >> level
+
+    def empty(self, level=0, dtype=torch.float64):
+        return torch.empty(self.rows(level), dtype=dtype, device=self.device)
+
+    def zeros(self, level=0, dtype=torch.float64):
+        return torch.zeros(self.rows(level), dtype=dtype, device=self.device)
+
+    # ----------------------------------------------------------- set-up
+    def generate(self, kind="hpcg", seed=0, sigma=0.0):
+        code = {"hpcg": _lib.GEN_HPCG, "varcoef": _lib.GEN_VARCOEF}[kind]
+        check(lib().hpcgx_generate(self.h, code, seed, float(sigma)))
+        return self
+
+    def load_level(self, level, nnz, cols, vals):
+        """Host matrix in the reference's contiguous 27-slot row layout."""
+        nnz = np.ascontiguousarray(nnz, np.uint8)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        check(lib().hpcgx_load_level(self.h, level, _ptr(nnz), _ptr(cols), _ptr(vals)))
+
+    def check_f2c(self, level, f2c):
+        f2c = np.ascontiguousarray(f2c, np.int32)
+        check(lib().hpcgx_check_f2c(self.h, level, _ptr(f2c), f2c.size))
+
+    def build_mixed(self):
+        check(lib().hpcgx_build_mixed(self.h))
+
+    def set_diagonal(self, level, diag):
+        d = np.ascontiguousarray(diag, np.float64)
+        check(lib().hpcgx_set_diagonal_host(self.h, level, _ptr(d)))
+
+    def get_diagonal(self, level=0):
+        d = np.zeros(self.rows(level))
+        check(lib().hpcgx_get_diagonal_host(self.h, level, _ptr(d)))
+        return d
+
+    def set_values(self, vals27, level=0, recoarsen=False):
+        self._pre()
+        v = vals27.contiguous()
+        check(lib().hpcgx_set_values(self.h, level, _ptr(v), int(recoarsen)))
+
+    def get_values(self, level=0):
+        self._pre()
+        n = self.rows(level)
+        v = torch.empty(n * STENCIL, dtype=torch.float64, device=self.device)
+        c = torch.empty(n * STENCIL, dtype=torch.int32, device=self.device)
+        check(lib().hpcgx_get_values(self.h, level, _ptr(v), _ptr(c)))
+        return v.view(n, STENCIL), c.view(n, STENCIL)
+
+    def memory_bytes(self):
+        b = C.c_double()
+        check(lib().hpcgx_memory_bytes(self.h, C.byref(b)))
+        return b.value
+
+    # ----------------------------------------------------------- operators
+    def spmv(self, x, level=0, y=None):
+        self._pre()
+        y = self.empty(level) if y is None else y
+        check(lib().hpcgx_spmv(self.h, level, _ptr(x), _ptr(y)))
+        return y
+
+    def symgs(self, r, x, level=0):
+        """One symmetric Gauss-Seidel sweep, x updated in place."""
+        self._pre()
+        check(lib().hpcgx_symgs(self.h, level, _ptr(r), _ptr(x)))
+        return x
+
+    def mg(self, r, x=None):
+        self._pre()
+        x = self.empty(0) if x is None else x
+        check(lib().hpcgx_mg(self.h, _ptr(r), _ptr(x)))
+        return x
+
+    def restriction(self, level, rf, Axf):
+        self._pre()
+        rc = self.empty(level + 1)
+        check(lib().hpcgx_restriction(self.h, level, _ptr(rf), _ptr(Axf), _ptr(rc)))
+        return rc
+
+    def prolongation(self, level, xc, xf):
+        self._pre()
+        check(lib().hpcgx_prolongation(self.h, level, _ptr(xc), _ptr(xf)))
+        return xf
+
+    def dot(self, x, y):
+        self._pre()
+        out = C.c_double()
+        check(lib().hpcgx_dot(self.h, x.numel(), _ptr(x), _ptr(y), C.byref(out)))
+        return out.value
+
+    def waxpby(self, alpha, x, beta, y, w=None):
+        self._pre()
+        w = torch.empty_like(x) if w is None else w
+        check(lib().hpcgx_waxpby(self.h, x.numel(), float(alpha), _ptr(x), float(beta), _ptr(y),
+                                 _ptr(w)))
+        return w
+
+    def residual(self, v1, v2):
+        self._pre()
+        out = C.c_double()
+        check(lib().hpcgx_residual(self.h, v1.numel(), _ptr(v1), _ptr(v2), C.byref(out)))
+        return out.value
+
+    # mixed precision --------------------------------------------------
+    def spmv_mixed(self, x32, level=0):
+        self._pre()
+        y = self.empty(level, torch.float32)
+        check(lib().hpcgx_spmv_mixed(self.h, level, _ptr(x32), _ptr(y)))
+        return y
+
+    def symgs_mixed(self, r, x32, level=0):
+        self._pre()
+        r64 = r if r.dtype == torch.float64 else None
+        r32 = r if r.dtype == torch.float32 else None
+        check(lib().hpcgx_symgs_mixed(self.h, level, _ptr(r64), _ptr(r32), _ptr(x32)))
+        return x32
+
+    def mg_mixed(self, r, x32=None):
+        self._pre()
+        x32 = self.empty(0, torch.float32) if x32 is None else x32
+        check(lib().hpcgx_mg_mixed(self.h, _ptr(r), _ptr(x32)))
+        return x32
+
+    # ----------------------------------------------------------- solvers
+    def cg(self, b, x, max_iter, tol, precond=True, times=None):
+        """Returns (niters, normr, normr0); x is updated in place."""
+        self._pre()
+        it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
+        tp = _ptr(times) if times is not None else None
+        check(lib().hpcgx_cg(self.h, _ptr(b), _ptr(x), int(max_iter), float(tol), int(precond),
+                             C.byref(it), C.byref(nr), C.byref(nr0), tp))
+        return it.value, nr.value, nr0.value
+
+    def cg_mixed(self, b, x, max_iter, tol, times=None):
+        self._pre()
+        it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
+        tp = _ptr(times) if times is not None else None
+        check(lib().hpcgx_cg_mixed(self.h, _ptr(b), _ptr(x), int(max_iter), float(tol),
+                                   C.byref(it), C.byref(nr), C.byref(nr0), tp))
+        return it.value, nr.value, nr0.value
+
+    def cg_host(self, b_host, x_host, max_iter, tol, mixed=False, times=None):
+        """Solve from host buffers (numpy or pinned CPU tensors); x_host updated."""
+        self._pre()
+        it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
+        tp = _ptr(times) if times is not None else None
+        check(lib().hpcgx_cg_host(self.h, int(mixed), _ptr(b_host), _ptr(x_host), int(max_iter),
+                                  float(tol), C.byref(it), C.byref(nr), C.byref(nr0), tp))
+        return it.value, nr.value, nr0.value
+
+    # ----------------------------------------------------------- adjoint
+    def adjoint_grad(self, lam, x):
+        self._pre()
+        n = self.rows(0)
+        g = torch.empty(n * STENCIL, dtype=torch.float64, device=self.device)
+        check(lib().hpcgx_adjoint_grad(self.h, _ptr(lam), _ptr(x), _ptr(g)))
+        return g.view(n, STENCIL)
+
+    # ----------------------------------------------------------- inputs
+    def fill_uniform(self, seed, lo=0.0, hi=1.0, n=None):
+        self._pre()
+        n = self.rows(0) if n is None else n
+        v = torch.empty(n, dtype=torch.float64, device=self.device)
+        check(lib().hpcgx_fill_uniform(self.h, n, seed, float(lo), float(hi), _ptr(v)))
+        return v
+
+    def fill_normal(self, seed, offset=0, n=None):
+        self._pre()
+        n = self.rows(0) if n is None else n
+        v = torch.empty(n, dtype=torch.float64, device=self.device)
+        check(lib().hpcgx_fill_normal(self.h, n, seed, offset, _ptr(v)))
+        return v
+
+    # ----------------------------------------------------------- measurement
+    def set_probe(self, probe):
+        check(lib().hpcgx_set_probe(self.h, int(probe)))
+
+    def probe_read(self, reset=True):
+        ms, n, b = C.c_double(), C.c_int64(), C.c_double()
+        check(lib().hpcgx_probe_read(self.h, C.byref(ms), C.byref(n), C.byref(b), int(reset)))
+        return ms.value, n.value, b.value
+
+    def launch_count(self):
+        return int(lib().hpcgx_launch_count(self.h))
+
+    def synchronize(self):
+        check(lib().hpcgx_synchronize(self.h))

@@ -1,0 +1,185 @@
+/*
+ * hpcgx.h -- C ABI of libhpcgx, the B200 (sm_100a) implementation of HPCG 3.1's
+ * multigrid-preconditioned CG iteration.
+ *
+ * Every function returns an int status: HPCGX_OK (0) on success, non-zero on
+ * error, which is the convention of the reference's operator API (callers
+ * count errors and carry on, src/main.cpp:190-192).  hpcgx_last_error() gives
+ * the message of the last failure on the calling thread.
+ *
+ * Pointers named *_host are host memory; every other vector pointer is device
+ * memory of the problem's GPU.  Vectors are in the reference's natural row
+ * order (row = iz*nx*ny + iy*nx + ix).  Calls are synchronous with respect to
+ * the host unless stated otherwise.
+ *
+ * The C++ drop-in files in hpcg_b200/dropin/ implement the reference's
+ * replaceable operator files on top of this ABI; each entry below names the
+ * reference interface it serves.
+ */
+#ifndef HPCGX_H
+#define HPCGX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPCGX_OK 0
+#define HPCGX_EINVAL 1     /* bad argument or size                       */
+#define HPCGX_ECUDA 2      /* a CUDA call failed                          */
+#define HPCGX_ESTATE 3     /* call out of order (e.g. no matrix loaded)   */
+#define HPCGX_ENONFINITE 4 /* CG met a non-finite residual norm           */
+#define HPCGX_ELAYOUT 5    /* matrix is not a 27-point stencil matrix     */
+#define HPCGX_ENOMEM 6     /* device allocation failed                    */
+
+#define HPCGX_GEN_HPCG 0    /* the reference problem: 26 / -1 stencil     */
+#define HPCGX_GEN_VARCOEF 1 /* variable-coefficient SPD stencil           */
+
+typedef struct hpcgx_problem hpcgx_problem;
+
+const char *hpcgx_last_error(void);
+int hpcgx_version(void);
+
+/* ---- problem set-up: OptimizeProblem (src/OptimizeProblem.hpp:22) ------ */
+
+/* Creates the device structures of an nx*ny*nz grid with `levels` multigrid
+ * levels (the reference uses 4, src/main.cpp:139; every level but the last
+ * needs even dimensions, src/GenerateCoarseProblem.cpp:52).  Allocates the
+ * matrix storage and work vectors; no values yet. */
+int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem **out);
+int hpcgx_destroy(hpcgx_problem *p);
+
+/* Loads one level from a host matrix in the reference's contiguous row
+ * layout (src/GenerateProblem_ref.cpp:113-124): row i owns entries
+ * [27 i, 27 i + nnz[i]) of cols / vals.  Entries must be stencil neighbours of
+ * row i in the level's geometry, in increasing stencil order as the reference
+ * generator emits them.  Replaces the data movement of OptimizeProblem. */
+int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz_host,
+                     const int32_t *cols_host, const double *vals_host);
+/* Same from the row-pointer arrays a SparseMatrix holds
+ * (nonzerosInRow, mtxIndL, matrixValues; src/SparseMatrix.hpp:47-50). */
+int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz_host,
+                          const int32_t *const *cols_host, const double *const *vals_host);
+/* Checks that a level's injection operator (MGData::f2cOperator,
+ * src/MGData.hpp:31) is the geometric injection the kernels use. */
+int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c_host, int64_t nc);
+/* Writes the matrix of every level on the device: HPCGX_GEN_HPCG is
+ * GenerateProblem_ref's matrix (src/GenerateProblem_ref.cpp:152-172) on each
+ * level as GenerateCoarseProblem builds it; HPCGX_GEN_VARCOEF draws
+ * a_ij = -exp(sigma z), z ~ N(0,1) per edge, diagonal sum|a_ij| + 2 (no
+ * reference counterpart). */
+int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma);
+/* Builds (or refreshes) the BF16 value copies used by the mixed solver. */
+int hpcgx_build_mixed(hpcgx_problem *p);
+/* Coherence with ReplaceMatrixDiagonal (src/SparseMatrix.hpp:139-145):
+ * writes level `level`'s diagonal from host memory. */
+int hpcgx_set_diagonal_host(hpcgx_problem *p, int level, const double *diag_host);
+int hpcgx_get_diagonal_host(hpcgx_problem *p, int level, double *diag_host);
+/* Level values in natural row order, 27 stencil slots per row
+ * (slot (dz+1)*9+(dy+1)*3+(dx+1)); device pointers.  set_values ignores
+ * slots without a neighbour; with recoarsen != 0 the coarse levels are
+ * rebuilt from the new finest values (variable-coefficient rule). */
+int hpcgx_set_values(hpcgx_problem *p, int level, const double *vals27, int recoarsen);
+int hpcgx_get_values(hpcgx_problem *p, int level, double *vals27, int32_t *cols27);
+/* Device memory held by the problem (OptimizeProblemMemoryUse,
+ * src/OptimizeProblem.hpp:28). */
+int hpcgx_memory_bytes(hpcgx_problem *p, double *bytes);
+int64_t hpcgx_rows(hpcgx_problem *p, int level);
+
+/* ---- operators (device vectors) ---------------------------------------- */
+
+/* ComputeSPMV (src/ComputeSPMV.hpp:20): y = A_level x. */
+int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y);
+/* ComputeSYMGS (src/ComputeSYMGS.hpp:20): one symmetric Gauss-Seidel sweep in
+ * colour order (forward colours 0..7, backward 7..0), x updated in place. */
+int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x);
+/* ComputeMG (src/ComputeMG.hpp:20): one V-cycle from the finest level,
+ * x = M^{-1} r (x is overwritten, not read). */
+int hpcgx_mg(hpcgx_problem *p, const double *r, double *x);
+/* ComputeRestriction_ref / ComputeProlongation_ref
+ * (src/ComputeRestriction_ref.hpp, src/ComputeProlongation_ref.hpp) of
+ * level -> level+1. */
+int hpcgx_restriction(hpcgx_problem *p, int level, const double *rf, const double *Axf,
+                      double *rc);
+int hpcgx_prolongation(hpcgx_problem *p, int level, const double *xc, double *xf);
+/* ComputeDotProduct (src/ComputeDotProduct.hpp:18); result to host. */
+int hpcgx_dot(hpcgx_problem *p, int64_t n, const double *x, const double *y,
+              double *result_host);
+/* ComputeWAXPBY (src/ComputeWAXPBY.hpp:18): w = alpha x + beta y. */
+int hpcgx_waxpby(hpcgx_problem *p, int64_t n, double alpha, const double *x, double beta,
+                 const double *y, double *w);
+/* ComputeResidual (src/ComputeResidual.hpp:18): max_i |v1_i - v2_i|. */
+int hpcgx_residual(hpcgx_problem *p, int64_t n, const double *v1, const double *v2,
+                   double *result_host);
+
+/* Mixed-precision operators (BF16 values, FP32 vectors; no reference
+ * counterpart): y = A x, one symmetric sweep with an FP64 (r64) or FP32 (r32)
+ * right-hand side, and the FP32 V-cycle of an FP64 residual. */
+int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y);
+int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const float *r32,
+                      float *x);
+int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x);
+
+/* ---- solvers ------------------------------------------------------------ */
+
+/* CG (src/CG.hpp:22-24) on device vectors: b read, x initial guess in and
+ * solution out; stops when normr/normr0 <= tolerance or after max_iter
+ * iterations.  times[0] += wall time, times[2] += vector ops, times[3] +=
+ * SpMV, times[5] += preconditioner (CUDA events); NULL is allowed.
+ * Returns HPCGX_ENONFINITE if a residual norm became NaN/Inf. */
+int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
+             int precond, int *niters, double *normr, double *normr0, double *times);
+/* Flexible CG in FP64 with the FP32/BF16 V-cycle as preconditioner and the
+ * Polak-Ribiere beta (no reference counterpart). */
+int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter,
+                   double tolerance, int *niters, double *normr, double *normr0,
+                   double *times);
+/* The same solves from host buffers (pinned memory gives full copy speed):
+ * b_host and x_host are copied to the device, solved, and x copied back. */
+int hpcgx_cg_host(hpcgx_problem *p, int mixed, const double *b_host, double *x_host,
+                  int max_iter, double tolerance, int *niters, double *normr,
+                  double *normr0, double *times);
+
+/* ---- differentiable solve (no reference counterpart) ------------------- */
+
+/* grad[27 i + s] = -lambda_i x_{col(i,s)} for the finest level, natural row
+ * order and stencil slots (0 where the slot has no neighbour): the gradient
+ * of L with respect to the stored values when A lambda = dL/dx. */
+int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, double *grad);
+
+/* ---- seeded inputs ------------------------------------------------------ */
+
+/* v_i = lo + (hi - lo) u(seed, i), u = 53-bit SplitMix64 counter draw. */
+int hpcgx_fill_uniform(hpcgx_problem *p, int64_t n, uint64_t seed, double lo, double hi,
+                       double *v);
+/* v_i = Box-Muller normal of draws 2(offset+i), 2(offset+i)+1. */
+int hpcgx_fill_normal(hpcgx_problem *p, int64_t n, uint64_t seed, uint64_t offset, double *v);
+
+/* ---- measurement -------------------------------------------------------- */
+
+#define HPCGX_PROBE_NONE 0
+#define HPCGX_PROBE_GS_FINE 1   /* every finest-level Gauss-Seidel class launch */
+#define HPCGX_PROBE_SPMV_FINE 2 /* the CG SpMV (with fused p.Ap)                */
+/* Brackets the selected launches inside the solvers' CUDA graphs with CUDA
+ * events; hpcgx_probe_read returns their summed device time, launch count
+ * and algorithmic bytes (compulsory traffic: real nonzeros, no padding)
+ * since the last reset.  Events are read at every host check of the solver,
+ * so solvers run with one iteration between checks while a probe is set. */
+int hpcgx_set_probe(hpcgx_problem *p, int probe);
+int hpcgx_probe_read(hpcgx_problem *p, double *ms, int64_t *launches, double *bytes, int reset);
+/* Kernel launches issued by the library on this problem since creation. */
+int64_t hpcgx_launch_count(hpcgx_problem *p);
+/* Waits for all work of the problem's stream. */
+int hpcgx_synchronize(hpcgx_problem *p);
+/* Makes the library launch on `stream` (a cudaStream_t of the problem's
+ * device, not the legacy default stream, since solvers capture CUDA graphs);
+ * NULL returns to the problem's own stream.  Lets a caller order library
+ * work with its own kernels and time it with events on that stream. */
+int hpcgx_set_stream(hpcgx_problem *p, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPCGX_H */

@@ -1,0 +1,70 @@
+"""The C-ABI library loads on a machine without a GPU and exports exactly the
+functions include/hpcgx.h declares; without a device it fails with a status
+code, never a crash.  No compute call is made here."""
+import ctypes as C
+import os
+import re
+
+import pytest
+import torch
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "hpcgx.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(hpcgx_\w+)\s*\(", text))
+
+
+def test_header_declares_the_operator_set():
+    names = declared()
+    for f in ("hpcgx_cg", "hpcgx_spmv", "hpcgx_symgs", "hpcgx_mg", "hpcgx_dot", "hpcgx_waxpby",
+              "hpcgx_residual", "hpcgx_restriction", "hpcgx_prolongation", "hpcgx_create",
+              "hpcgx_load_level_rows", "hpcgx_cg_mixed", "hpcgx_adjoint_grad"):
+        assert f in names
+
+
+def test_library_exports_every_declared_symbol():
+    from hpcg_b200 import _lib
+    h = _lib.lib()
+    for name in declared():
+        assert hasattr(h, name), name
+    assert set(_lib.SIGNATURES) == declared()
+    assert h.hpcgx_version() >= 1
+
+
+def test_library_is_sm100a_only():
+    """The fatbin is built for sm_100a (checked from the build recipe, not by
+    reading the binary)."""
+    from hpcg_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="checks the no-GPU error path")
+def test_create_without_gpu_returns_status():
+    from hpcg_b200 import _lib
+    h = C.c_void_p()
+    rc = _lib.lib().hpcgx_create(0, 16, 16, 16, 4, C.byref(h))
+    assert rc == 2 and not h.value
+    assert _lib.lib().hpcgx_last_error()
+
+
+def test_bad_arguments_rejected_before_any_device_work():
+    from hpcg_b200 import _lib
+    h = C.c_void_p()
+    assert _lib.lib().hpcgx_create(0, 15, 16, 16, 4, C.byref(h)) == 1   # odd: cannot coarsen
+    assert _lib.lib().hpcgx_create(0, 16, 16, 16, 5, C.byref(h)) == 1   # > 4 levels
+    assert _lib.lib().hpcgx_create(0, 0, 16, 16, 1, C.byref(h)) == 1
+    assert _lib.lib().hpcgx_spmv(None, 0, None, None) == 1
+    assert b"null problem" in _lib.lib().hpcgx_last_error()
+
+
+def test_product_fails_loudly_without_library(tmp_path, monkeypatch):
+    from hpcg_b200 import _lib
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
+    monkeypatch.setattr(_lib, "_lib", None)
+    with pytest.raises(ImportError):
+        _lib.lib()

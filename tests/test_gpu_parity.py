@@ -1,0 +1,360 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference's own outputs (golden vectors).
+
+Tolerances (written per assertion):
+  * SpMV, SYMGS, MG, restriction, prolongation, WAXPBY, residual norm: bit-exact
+    (``==``).  SYMGS / MG are compared with the reference's functions applied
+    to the colour-permuted matrix, as the device sweeps in colour order.
+  * dot products: 1e-13 relative.
+  * CG: identical iteration counts; residual norms 1e-8 relative after 10
+    iterations (dot products round differently, so trajectories drift slowly).
+  * Mixed precision (BF16 values, FP32 vectors): bit-exact against the
+    oracle's FP32 restatement; the flexible CG to the same iteration count.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN_GRIDS, load_golden
+
+pytestmark = pytest.mark.gpu
+
+GRIDS = GOLDEN_GRIDS + [(32, 32, 32), (24, 24, 24), (64, 32, 16)]
+
+
+def ids(d):
+    return "x".join(map(str, d))
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+_cache = {}
+
+
+def setup(dims, oracle, source="load"):
+    """Oracle hierarchy + a GPU problem built from it (load) or on the device (generate)."""
+    key = (dims, source)
+    if key in _cache:
+        return _cache[key]
+    from hpcg_b200 import Problem
+    L, b, x, xe = oracle.hierarchy(*dims)
+    oracle.colour_order(L)
+    P = Problem(*dims)
+    if source == "load":
+        for l, lev in enumerate(L):
+            P.load_level(l, lev.nnz, lev.cols, lev.vals)
+            if lev.f2c is not None:
+                P.check_f2c(l, lev.f2c)
+    else:
+        P.generate("hpcg")
+    _cache[key] = (L, b, xe, P)
+    return _cache[key]
+
+
+@pytest.fixture(scope="module", params=GRIDS, ids=ids)
+def grid(request, oracle):
+    return request.param
+
+
+def seeded(oracle, n):
+    return oracle.uniform(11, n, 1.0, 2.0), oracle.uniform(12, n), oracle.uniform(13, n)
+
+
+def test_device_generator_matches_host_load(grid, oracle):
+    _, _, _, P1 = setup(grid, oracle, "load")
+    _, _, _, P2 = setup(grid, oracle, "generate")
+    for l in range(4):
+        v1, c1 = P1.get_values(l)
+        v2, c2 = P2.get_values(l)
+        assert torch.equal(v1, v2) and torch.equal(c1, c2)
+
+
+def test_spmv_bitexact(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    u, _, _ = seeded(oracle, L[0].nrow)
+    for l, lev in enumerate(L):
+        y = host(P.spmv(cuda(u[:lev.nrow]), level=l))
+        assert (y == oracle.spmv(lev, u[:lev.nrow])).all()
+
+
+def test_symgs_bitexact_colour_order(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    _, r, x0 = seeded(oracle, L[0].nrow)
+    for l, lev in enumerate(L):
+        n = lev.nrow
+        x = cuda(x0[:n])
+        P.symgs(cuda(r[:n]), x, level=l)
+        assert (host(x) == oracle.symgs(lev, r[:n], x0[:n], coloured=True)).all()
+
+
+def test_mg_bitexact_colour_order(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    _, r, _ = seeded(oracle, L[0].nrow)
+    z = host(P.mg(cuda(r)))
+    assert (z == oracle.mg(L, r, coloured=True)).all()
+    # calling again must not depend on leftovers in the work vectors
+    assert (host(P.mg(cuda(r))) == z).all()
+
+
+def test_against_reference_golden(oracle):
+    for dims in GOLDEN_GRIDS:
+        g = load_golden(dims)
+        L, b, xe, P = setup(dims, oracle)
+        u, r, x0 = seeded(oracle, L[0].nrow)
+        for l, lev in enumerate(L):
+            n = lev.nrow
+            assert (host(P.spmv(cuda(u[:n]), level=l)) == g["spmv_L%d" % l]).all()
+            x = cuda(x0[:n])
+            P.symgs(cuda(r[:n]), x, level=l)
+            assert (host(x) == g["symgs_perm_L%d" % l]).all()
+        assert (host(P.mg(cuda(r))) == g["mg_perm"]).all()
+        assert (host(P.restriction(0, cuda(r), cuda(u))) == g["restriction_L0"]).all()
+        nc = L[1].nrow
+        assert (host(P.prolongation(0, cuda(u[:nc]), cuda(x0))) == g["prolongation_L0"]).all()
+        assert (host(P.waxpby(1.0, cuda(u), 0.37, cuda(r))) == g["waxpby_a1"]).all()
+        assert (host(P.waxpby(-0.61, cuda(u), 1.0, cuda(r))) == g["waxpby_b1"]).all()
+        assert (host(P.waxpby(0.83, cuda(u), -1.29, cuda(r))) == g["waxpby_ab"]).all()
+        assert P.residual(cuda(u), cuda(r)) == g["residual_ur"][0]
+        assert abs(P.dot(cuda(u), cuda(r)) / g["dot_ur"][0] - 1) < 1e-13
+        uu = cuda(u)
+        assert abs(P.dot(uu, uu) / g["dot_uu"][0] - 1) < 1e-13
+        # CG_ref on the colour-permuted matrix: same iteration count to 1e-10
+        x = torch.zeros(L[0].nrow, dtype=torch.float64, device="cuda")
+        k, nr, nr0 = P.cg(cuda(b), x, 10, 0.0)
+        gk, gnr, gnr0 = g["cg10_perm_stats"]
+        assert k == gk and abs(nr0 / gnr0 - 1) < 1e-14 and abs(nr / gnr - 1) < 1e-8
+        assert np.abs(host(x) - g["cg10_perm_x"]).max() < 1e-10
+        x.zero_()
+        k, nr, nr0 = P.cg(cuda(b), x, 500, 1e-10)
+        assert k == g["cgtol_perm_stats"][0] and nr / nr0 <= 1e-10
+
+
+def test_restriction_prolongation_bitexact(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    u, r, x0 = seeded(oracle, L[0].nrow)
+    for l in range(3):
+        n, nc = L[l].nrow, L[l + 1].nrow
+        rc = host(P.restriction(l, cuda(r[:n]), cuda(u[:n])))
+        assert (rc == oracle.restriction(L[l].f2c, r[:n], u[:n])).all()
+        xf = host(P.prolongation(l, cuda(u[:nc]), cuda(x0[:n])))
+        assert (xf == oracle.prolongation(L[l].f2c, u[:nc], x0[:n])).all()
+
+
+def test_vector_ops(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    u, r, _ = seeded(oracle, L[0].nrow)
+    du, dr = cuda(u), cuda(r)
+    for a, bb in ((1.0, 0.37), (-0.61, 1.0), (0.83, -1.29), (1.0, 1.0), (0.0, -2.5)):
+        assert (host(P.waxpby(a, du, bb, dr)) == oracle.waxpby(a, u, bb, r)).all()
+    # in-place aliasing w == x and w == y, as CG uses it (src/CG.cpp:115,121-122)
+    w = du.clone()
+    P.waxpby(1.0, w, 0.5, dr, w=w)
+    assert (host(w) == oracle.waxpby(1.0, u, 0.5, r)).all()
+    assert abs(P.dot(du, dr) / oracle.dot(u, r) - 1) < 1e-13
+    assert abs(P.dot(du, du) / oracle.dot(u, u) - 1) < 1e-13
+    assert P.residual(du, dr) == oracle.residual(u, r)
+    # deterministic: the same reduction twice gives the same bits
+    assert P.dot(du, dr) == P.dot(du, dr)
+
+
+def test_cg_matches_oracle(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    n = L[0].nrow
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    k, nr, nr0 = P.cg(cuda(b), x, 10, 0.0)
+    ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 10, 0.0, coloured=True)
+    assert k == ok == 10
+    assert abs(nr0 / onr0 - 1) < 1e-14 and abs(nr / onr - 1) < 1e-8
+    x.zero_()
+    k, nr, nr0 = P.cg(cuda(b), x, 500, 1e-10)
+    ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 500, 1e-10, coloured=True)
+    assert k == ok and nr / nr0 <= 1e-10
+    assert np.abs(host(x) - 1.0).max() < 1e-6        # xexact = 1
+    # unpreconditioned
+    x.zero_()
+    k, nr, nr0 = P.cg(cuda(b), x, 30, 0.0, precond=False)
+    ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 30, 0.0, precond=False)
+    assert k == ok and abs(nr / onr - 1) < 1e-6
+
+
+def test_testcg_spectral(grid, oracle):
+    """TestCG (src/TestCG.cpp:62-115): diagonal x1e6 through the host
+    diagonal path, <= 12 unpreconditioned / <= 2 preconditioned iterations,
+    then the diagonal is restored."""
+    L, b, xe, P = setup(grid, oracle)
+    n = L[0].nrow
+    scale = np.full(n, 1.0e6)
+    scale[:9] = (np.arange(9) + 2) * 1.0e6
+    d0 = P.get_diagonal(0)
+    P.set_diagonal(0, d0 * scale)
+    try:
+        for prec, limit in ((False, 12), (True, 2)):
+            for _ in range(2):
+                x = torch.zeros(n, dtype=torch.float64, device="cuda")
+                k, nr, nr0 = P.cg(cuda(b * scale), x, 50, 1e-12, precond=prec)
+                assert k <= limit
+    finally:
+        P.set_diagonal(0, d0)
+    assert (P.get_diagonal(0) == d0).all()
+
+
+def test_testsymmetry(grid, oracle):
+    """TestSymmetry (src/TestSymmetry.cpp:76-132) through the operators."""
+    L, b, xe, P = setup(grid, oracle)
+    n = L[0].nrow
+    xv, yv = cuda(oracle.uniform(21, n, 1.0, 2.0)), cuda(oracle.uniform(22, n, 1.0, 2.0))
+    eps, anorm = np.finfo(float).eps, 52.0
+    xn, yn = P.dot(xv, xv), P.dot(yv, yv)
+    denom = (xn * anorm * yn + yn * anorm * xn) * eps
+    xtAy = P.dot(xv, P.spmv(yv))
+    ytAx = P.dot(yv, P.spmv(xv))
+    assert abs(xtAy - ytAx) / denom <= 1.0
+    xtMy = P.dot(xv, P.mg(yv))
+    ytMx = P.dot(yv, P.mg(xv))
+    assert abs(xtMy - ytMx) / denom <= 1.0
+    assert P.residual(P.spmv(cuda(xe)), cuda(b)) == 0.0
+
+
+def test_mixed_bitexact(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    u, r, x0 = seeded(oracle, L[0].nrow)
+    P.build_mixed()
+    for l, lev in enumerate(L):
+        n = lev.nrow
+        u32 = u[:n].astype(np.float32)
+        assert (host(P.spmv_mixed(cuda(u32), level=l)) == oracle.spmv32(lev, u32)).all()
+        x32 = x0[:n].astype(np.float32)
+        rr = r[:n] if l == 0 else r[:n].astype(np.float32)
+        xd = cuda(x32)
+        P.symgs_mixed(cuda(rr), xd, level=l)
+        assert (host(xd) == oracle.symgs32(lev, rr, x32)).all()
+    assert (host(P.mg_mixed(cuda(r))) == oracle.mg32(L, r)).all()
+
+
+def test_mixed_cg(grid, oracle):
+    L, b, xe, P = setup(grid, oracle)
+    n = L[0].nrow
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    k, nr, nr0 = P.cg_mixed(cuda(b), x, 500, 1e-10)
+    ox, ok, onr, onr0 = oracle.fcg(L, b, np.zeros(n), 500, 1e-10)
+    assert k == ok and nr / nr0 <= 1e-10
+    # the recursive residual is honest: true FP64 residual of the result
+    rt = np.linalg.norm(host(cuda(b) - P.spmv(x))) / np.linalg.norm(b)
+    assert rt < 1e-9
+    assert np.abs(host(x) - 1.0).max() < 1e-6
+
+
+def test_cg_host_buffers(oracle):
+    dims = (32, 32, 32)
+    L, b, xe, P = setup(dims, oracle)
+    n = L[0].nrow
+    bh = torch.from_numpy(b.copy()).pin_memory()
+    for mixed in (False, True):
+        xh = torch.zeros(n, dtype=torch.float64).pin_memory()
+        k, nr, nr0 = P.cg_host(bh.numpy(), xh.numpy(), 200, 1e-10, mixed=mixed)
+        assert nr / nr0 <= 1e-10 and np.abs(xh.numpy() - 1.0).max() < 1e-6
+
+
+def test_varcoef_generator_and_kernels(oracle):
+    from hpcg_b200 import Problem
+    dims = (32, 16, 16)
+    L, _, _, _ = oracle.hierarchy(*dims, varcoef=(2, 0.5))
+    oracle.colour_order(L)
+    P = Problem(*dims)
+    P.generate("varcoef", seed=2, sigma=0.5)
+    for l, lev in enumerate(L):
+        v, c = P.get_values(l)
+        v = host(v)
+        # oracle layout is packed; map to stencil slots via columns
+        n = lev.nrow
+        ix = np.arange(n) % lev.nx
+        iy = (np.arange(n) // lev.nx) % lev.ny
+        iz = np.arange(n) // (lev.nx * lev.ny)
+        for j in range(27):
+            m = j < lev.nnz
+            col = lev.cols[np.arange(n) * 27 + j]
+            dx = col % lev.nx - ix
+            dy = (col // lev.nx) % lev.ny - iy
+            dz = col // (lev.nx * lev.ny) - iz
+            s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1)
+            ov = lev.vals[np.arange(n) * 27 + j]
+            dv = v[np.arange(n)[m], s[m]]
+            assert np.allclose(dv, ov[m], rtol=1e-14, atol=0)
+    # kernels on the host-loaded variable-coefficient hierarchy: bit-exact
+    Q = Problem(*dims)
+    for l, lev in enumerate(L):
+        Q.load_level(l, lev.nnz, lev.cols, lev.vals)
+    _, r, x0 = seeded(oracle, L[0].nrow)
+    assert (host(Q.mg(cuda(r))) == oracle.mg(L, r, coloured=True)).all()
+    # coarse levels rebuilt from the finest values equal direct generation
+    v0, _ = P.get_values(0)
+    R = Problem(*dims)
+    R.generate("varcoef", seed=99, sigma=0.5)
+    R.set_values(v0.reshape(-1), level=0, recoarsen=True)
+    for l in range(4):
+        assert torch.equal(R.get_values(l)[0], P.get_values(l)[0])
+
+
+def test_large_grid_properties():
+    """At a size the oracle cannot check quickly: exact A*1 = b, symmetry, and
+    convergence of both solvers to 1e-10."""
+    from hpcg_b200 import Problem
+    dims = (128, 128, 128)
+    P = Problem(*dims)
+    P.generate("hpcg")
+    n = P.rows()
+    ones = torch.ones(n, dtype=torch.float64, device="cuda")
+    # nnz of a row = product over axes of 3 (interior) or 2 (boundary);
+    # b = 26 - (nnz - 1) (src/GenerateProblem_ref.cpp:178) must equal A*1 exactly
+    def per_axis(m):
+        c = torch.full((m,), 3.0, dtype=torch.float64, device="cuda")
+        c[0] = c[-1] = 2.0
+        return c
+    nnz = (per_axis(dims[2])[:, None, None] * per_axis(dims[1])[None, :, None] *
+           per_axis(dims[0])[None, None, :]).reshape(-1)
+    b = 26.0 - (nnz - 1.0)
+    Ax = P.spmv(ones)
+    assert P.residual(Ax, b) == 0.0
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    k64, nr, nr0 = P.cg(b, x, 500, 1e-10)
+    assert nr / nr0 <= 1e-10
+    x.zero_()
+    k32, nr, nr0 = P.cg_mixed(b, x, 500, 1e-10)
+    assert nr / nr0 <= 1e-10 and k32 <= k64 + 2
+    rt = (torch.linalg.norm(b - P.spmv(x)) / torch.linalg.norm(b)).item()
+    assert rt < 1e-9
+
+
+def test_error_paths(oracle):
+    from hpcg_b200 import HPCGXError, Problem
+    P = Problem(16, 16, 16)
+    r = torch.zeros(P.rows(), dtype=torch.float64, device="cuda")
+    with pytest.raises(HPCGXError) as e:
+        P.mg(r)                                   # no matrix yet
+    assert e.value.code == 3
+    L, b, _, _ = oracle.hierarchy(16, 16, 16)
+    bad = L[0].cols.copy()
+    bad[27 * 5] = 4000                            # not a neighbour of row 5
+    with pytest.raises(HPCGXError) as e:
+        P.load_level(0, L[0].nnz, bad, L[0].vals)
+    assert e.value.code == 5
+    with pytest.raises(HPCGXError) as e:
+        P.check_f2c(0, L[0].f2c[::-1].copy())
+    assert e.value.code == 5
+    P.generate("hpcg")
+    bn = cuda(b.copy())
+    bn[7] = float("nan")
+    x = torch.zeros_like(bn)
+    with pytest.raises(HPCGXError) as e:
+        P.cg(bn, x, 50, 1e-10)
+    assert e.value.code == 4
+    # the problem stays usable after the failed solve
+    x.zero_()
+    k, nr, nr0 = P.cg(cuda(b), x, 50, 1e-10)
+    assert nr / nr0 <= 1e-10
