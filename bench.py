@@ -1,0 +1,382 @@
+"""Benchmark: time to FP64 relative residual 1e-10, mixed vs FP64 PCG, on B200.
+
+Workload (one "step" = one solve): the HPCG 27-point problem on a 512^3 grid
+(134M rows, 3.6e9 nonzeros), 4-level multigrid, 8-colour Gauss-Seidel;
+b = A u with u ~ U(-1, 1) (SplitMix64 seed 1), x0 = 0; solved to
+||r||/||r0|| <= 1e-10 by the mixed-precision flexible PCG (FP32/BF16 V-cycle
+inside FP64 CG).  The plain FP64 PCG solve of the same system is timed beside
+it for the mixed-vs-FP64 comparison.  Inputs are generated on the device
+(synthetic, as HPCG generates its own problem).
+
+  value        seconds per mixed solve (mean of --steps timed solves), lower is better
+  e2e          the same through the C ABI from pinned host buffers (b and x0
+               copied in, x copied out inside the timed region)
+  roofline     finest-level Gauss-Seidel class kernel (the dominant kernel):
+               algorithmic bytes / CUDA-event duration of every launch in the
+               timed region, against the measured HBM copy bandwidth
+  cpu_baseline the reference's own CG_ref (oracle/_ref, OpenMP on all host
+               cores) per-iteration time on a 128^3 sample, scaled to 512^3
+               rows and to the FP64 solve's iteration count
+
+Multi-GPU (torchrun): every rank solves its own 512^3 system (the path is
+replicated, not sharded, in this build); value is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to FP64 rel. residual 1e-10, mixed vs FP64 PCG on 1 B200; GFLOP/s; HBM %"
+TOL = 1e-10
+MAX_IT = 2000
+SEED_U = 1
+SMI_FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def model(dims, levels=4):
+    """HPCG's flop model (src/ReportResults.cpp:81-97) and the compulsory-byte
+    model per iteration: SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n, R+P 40 n_c,
+    CG vectors 112 n (FP64); the mixed V-cycle moves 6 B/nnz and FP32 vectors."""
+    def nnz(nx, ny, nz):
+        return (3 * nx - 2) * (3 * ny - 2) * (3 * nz - 2)
+    lv = [(dims[0] >> l, dims[1] >> l, dims[2] >> l) for l in range(levels)]
+    n = [a * b * c for a, b, c in lv]
+    z = [nnz(*d) for d in lv]
+    flops = 12 * n[0] + 2 * z[0] + sum(10 * z[l] for l in range(levels - 1)) + 4 * z[-1]
+    b64 = 12 * z[0] + 16 * n[0] + 112 * n[0]
+    b32 = b64
+    for l in range(levels):
+        sym64 = 24 * z[l] + 48 * n[l]
+        sym32 = 12 * z[l] + (32 if l == 0 else 24) * n[l]
+        if l < levels - 1:
+            b64 += 2 * sym64 + 12 * z[l] + 16 * n[l] + 40 * n[l + 1]
+            b32 += 2 * sym32 + 6 * z[l] + 8 * n[l] + 20 * n[l + 1]
+        else:
+            b64 += sym64
+            b32 += sym32
+    return flops, b64, b32, n[0], z[0]
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, path):
+        self.path = path
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + SMI_FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self, device_index):
+        if not self.proc:
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9 or p[0] != str(device_index):
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_sample(iters_512, dims, sample_n=128, sample_it=10):
+    """CG_ref of the reference build (oracle/_ref) on a sample_n^3 problem:
+    per-iteration time of a bounded run, scaled to dims rows and iters_512."""
+    from oracle.oracle import RefProblem, Oracle
+    if not RefProblem.available():
+        return None
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    ref = RefProblem(sample_n, sample_n, sample_n)
+    n = ref.rows(0)
+    u = Oracle.uniform(SEED_U, n, -1.0, 1.0)
+    b = ref.spmv(0, u)
+    t0 = time.perf_counter()
+    _, k, nr, nr0, _ = ref.cg(b, np.zeros(n), sample_it, 0.0)
+    dt = time.perf_counter() - t0
+    ref.close()
+    per_it = dt / k
+    scale = (dims[0] * dims[1] * dims[2]) / float(n)
+    value = per_it * scale * iters_512
+    return {"value": value, "unit": "s", "cores": int(os.environ.get("OMP_NUM_THREADS", threads)),
+            "kind": "reference",
+            "sample": "reference CG_ref (oracle/_ref, -O3 OpenMP, serial SYMGS as in "
+                      "src/ComputeSYMGS_ref.cpp) on %d^3, %d iterations in %.2f s = %.3f s/iter; "
+                      "scaled x%.0f rows to %dx%dx%d and x%d iterations (the FP64 solve's count)"
+                      % (sample_n, k, dt, per_it, scale, dims[0], dims[1], dims[2], iters_512)}
+
+
+def run_reference(args, dims):
+    """--impl reference: the reference's CPU path on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    iters = args.ref_iters
+    vals = []
+    cb = None
+    for _ in range(args.warmup):
+        if cpu_reference_sample(iters, dims, sample_n=args.ref_sample, sample_it=1) is None:
+            break
+    for _ in range(max(1, args.steps)):
+        cb = cpu_reference_sample(iters, dims, sample_n=args.ref_sample, sample_it=args.ref_sample_it)
+        if cb is None:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "oracle/_ref/libhpcgref.so not built (needs the "
+                                             "reference sources at build time)"}))
+            return
+        vals.append(cb["value"])
+    v = statistics.mean(vals)
+    out = {"metric": METRIC, "value": v, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3,
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+           "data": "synthetic (HPCG-generated problem, b = A u)",
+           "config": config(dims), "cpu_baseline": dict(cb, value=v),
+           "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def config(dims):
+    return {"workload": "HPCG %dx%dx%d (b = A u, u~U(-1,1) seed 1, x0 = 0): mixed-precision "
+                        "flexible PCG (FP32/BF16 V-cycle, FP64 outer) to FP64 rel. residual "
+                        "1e-10, compared with plain FP64 PCG" % dims,
+            "grid": list(dims), "levels": 4, "smoother": "8-colour symmetric Gauss-Seidel",
+            "tolerance": TOL, "l2": "no flush: every step streams > 60 GB, far above the 126 MB L2"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hpcgx", choices=["hpcgx", "reference"])
+    ap.add_argument("--grid", type=int, nargs="+", default=[512])
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--ref-iters", type=int, default=0,
+                    help="iterations the reference arm scales to (0: measured FP64 count)")
+    ap.add_argument("--ref-sample", type=int, default=128)
+    ap.add_argument("--ref-sample-it", type=int, default=10)
+    args = ap.parse_args()
+    g = args.grid
+    dims = (g[0], g[0], g[0]) if len(g) == 1 else tuple(g)
+
+    if args.impl == "reference":
+        if args.ref_iters <= 0:
+            args.ref_iters = REF_ITERS_DEFAULT.get(dims, 300)
+        run_reference(args, dims)
+        return
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local
+    torch.cuda.set_device(dev)
+
+    from hpcg_b200 import Problem
+    from hpcg_b200._lib import PROBE_GS_FINE
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    P = Problem(*dims, device=dev)
+    P.generate("hpcg")
+    P.build_mixed()
+    n = P.rows()
+    u = P.fill_uniform(SEED_U, -1.0, 1.0)
+    b = P.spmv(u)
+    x = torch.zeros(n, dtype=torch.float64, device=f"cuda:{dev}")
+    stream = P.stream
+
+    def solve(mixed):
+        x.zero_()
+        f = P.cg_mixed if mixed else P.cg
+        return f(b, x, MAX_IT, TOL)
+
+    # ---------------- warm-up (untimed)
+    for _ in range(args.warmup):
+        solve(True)
+    # ---------------- timed mixed solves
+    P.set_probe(PROBE_GS_FINE)
+    P.probe_read(reset=True)
+    barrier()
+    l0 = P.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    iters_mixed = []
+    clk = Clocks(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                              else "", "bench_clocks_rank%d.csv" % rank))
+    with clk:
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                ev[i][0].record(stream)
+            k, nr, nr0 = solve(True)
+            with torch.cuda.stream(stream):
+                ev[i][1].record(stream)
+            iters_mixed.append(k)
+        barrier()
+        wall = time.perf_counter() - t0
+    launches = P.launch_count() - l0
+    times = [a.elapsed_time(b_) * 1e-3 for a, b_ in ev]
+    probe_ms, probe_n, probe_bytes = P.probe_read(reset=True)
+    P.set_probe(0)
+    t_mixed = statistics.mean(times)
+    relres_mixed = nr / nr0
+    x_mixed = x.clone()
+    true_mixed = (torch.linalg.norm(b - P.spmv(x_mixed)) / torch.linalg.norm(b)).item()
+
+    # ---------------- FP64 comparison
+    solve(False)
+    t64 = []
+    for _ in range(max(1, args.fp64_steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        k64, nr64, nr064 = solve(False)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t64.append(e0.elapsed_time(e1) * 1e-3)
+    t_fp64 = statistics.mean(t64)
+    x64 = x.clone()
+    true_fp64 = (torch.linalg.norm(b - P.spmv(x64)) / torch.linalg.norm(b)).item()
+    x_diff = (torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item()
+    err_u = (torch.linalg.norm(x_mixed - u) / torch.linalg.norm(u)).item()
+
+    # ---------------- end to end through the C ABI from pinned host buffers
+    bh = b.cpu().pin_memory()
+    xh = torch.zeros(n, dtype=torch.float64).pin_memory()
+    barrier()
+    te = time.perf_counter()
+    ke, nre, nr0e = P.cg_host(bh.numpy(), xh.numpy(), MAX_IT, TOL, mixed=True)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - te
+
+    # ---------------- max over ranks
+    if dist:
+        tt = torch.tensor([t_mixed, t_fp64, t_e2e], device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_mixed, t_fp64, t_e2e = tt.tolist()
+
+    flops, b64, b32, n0, z0 = model(dims)
+    peak, peak_kind = peaks()
+    gf_mixed = flops * iters_mixed[-1] / t_mixed / 1e9
+    gf_fp64 = flops * k64 / t_fp64 / 1e9
+    hbm_mixed = b32 * iters_mixed[-1] / t_mixed / 1e9
+    hbm_fp64 = b64 * k64 / t_fp64 / 1e9
+    achieved = probe_bytes / (probe_ms * 1e-3) / 1e9 if probe_ms > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "gs_fine_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("bytes_per_launch_512")
+        except Exception:
+            traffic = None
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu:
+        try:
+            cpu = cpu_reference_sample(k64, dims)
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"unavailable": str(e)}
+    clocks = clk.summary(dev)
+    out = {
+        "metric": METRIC, "value": t_mixed, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp64 outer / fp32+bf16 V-cycle",
+        "data": "synthetic (HPCG-generated problem on the device, b = A u)",
+        "config": config(dims),
+        "iterations": {"mixed": iters_mixed[-1], "fp64": k64},
+        "fp64_time_s": t_fp64,
+        "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+        "fp64_rel_residual": {"mixed_recursive": relres_mixed, "mixed_true": true_mixed,
+                              "fp64_true": true_fp64},
+        "x_rel_diff_vs_fp64": x_diff, "x_rel_err_vs_u": err_u,
+        "gflops": {"mixed": gf_mixed, "fp64": gf_fp64, "model": "src/ReportResults.cpp:81-97"},
+        "hbm": {"mixed_gbs": hbm_mixed, "fp64_gbs": hbm_fp64, "mixed_frac": hbm_mixed / peak,
+                "fp64_frac": hbm_fp64 / peak, "peak_gbs": peak, "peak_kind": peak_kind},
+        "roofline": {"kernel": "k_gs_class (finest level, BF16/FP32, all modes)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "launches": probe_n, "peak_kind": peak_kind},
+        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8,
+                "d2h_bytes_per_step": n * 8},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "wall_s": wall,
+    }
+    print(json.dumps(out))
+    P.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+# Iterations the reference arm scales its per-iteration sample to when run on
+# its own: the FP64 PCG iteration count this build measured on the same
+# system (recorded by bench runs; the reference's natural-order smoother is
+# not run at 512^3 because its int32 counters overflow there).
+REF_ITERS_DEFAULT = {}
+
+
+if __name__ == "__main__":
+    main()

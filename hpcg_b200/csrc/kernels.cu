@@ -187,7 +187,7 @@ __device__ __forceinline__ RowId row_of(const ClassInfo &C, int nx, int ny, int 
 // (src/ComputeSPMV_ref.cpp:64-70).  With DOT, also reduces sum_i x_i y_i (the
 // p.Ap of CG, src/CG.cpp:119) and runs the finishing scalar step.
 template <class VT, class T, bool DOT>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, Reduce red,
        int fin, void *fin_target, const int *__restrict__ done) {
   if (done && *done) return;
@@ -204,15 +204,20 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
       const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
       const int64_t base = (id.k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (id.k & 31);
-      T sum = T(0);
-      T xrow = T(0);
+      int32_t col[HPCGX_STENCIL];
+      VT val[HPCGX_STENCIL];
 #pragma unroll
       for (int s = 0; s < HPCGX_STENCIL; ++s) {
-        const T v = to_arith(__ldg(A.vals + base + s * HPCGX_SLICE), T());
-        const T xv = __ldg(x + __ldg(A.cols + base + s * HPCGX_SLICE));
-        if (s == HPCGX_DIAG_SLOT) xrow = xv;
-        sum = rn_add(sum, rn_mul(v, xv));
+        col[s] = __ldg(A.cols + base + s * HPCGX_SLICE);
+        val[s] = __ldg(A.vals + base + s * HPCGX_SLICE);
       }
+      T xv[HPCGX_STENCIL];
+#pragma unroll
+      for (int s = 0; s < HPCGX_STENCIL; ++s) xv[s] = __ldg(x + col[s]);
+      T sum = T(0);
+#pragma unroll
+      for (int s = 0; s < HPCGX_STENCIL; ++s) sum = rn_add(sum, rn_mul(to_arith(val[s], T()), xv[s]));
+      const T xrow = xv[HPCGX_DIAG_SLOT];
       y[id.row] = sum;
       if (DOT) acc += (double)xrow * (double)sum;
     }
@@ -228,8 +233,12 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 // One Gauss-Seidel row update, src/ComputeSYMGS_ref.cpp:72-80:
 //   sum = r_i - sum_j a_ij x_j (diagonal included, slot order); sum += x_i a_ii;
 //   x_i = sum / a_ii.
+// The loads are issued in three stages (every column and value, then every
+// neighbour of x, then the arithmetic) so that a thread keeps ~54 independent
+// loads in flight instead of walking a chain of dependent ones.
 // ZERO: x is known to be zero for every colour above c and for row i itself
-//       (first forward sweep after ZeroVector); those terms are skipped, which
+//       (first forward sweep after ZeroVector); those terms, and the padding
+//       slots (column = row), are skipped.  Skipping a product with a zero
 //       changes nothing but possibly the sign of an exact zero.
 // PRO:  x_i first receives the prolongated coarse correction (colour 0).
 // RES:  after the update, the fine residual at this injected point is formed
@@ -239,6 +248,14 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
                                        T *__restrict__ rc) {
   const int64_t base = (id.k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (id.k & 31);
+  int32_t col[HPCGX_STENCIL];
+  VT val[HPCGX_STENCIL];
+#pragma unroll
+  for (int s = 0; s < HPCGX_STENCIL; ++s) {
+    if (ZERO && s != HPCGX_DIAG_SLOT && ((c ^ slot_mask(s)) > c)) continue;
+    val[s] = __ldg(A.vals + base + s * HPCGX_SLICE);
+    if (s != HPCGX_DIAG_SLOT) col[s] = __ldg(A.cols + base + s * HPCGX_SLICE);
+  }
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
   if (PRO || RES) {
@@ -247,19 +264,23 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   }
   T xi = ZERO ? T(0) : x[id.row];
   if (PRO) xi = rn_add(xi, __ldg(xc + crow));
-  T sum = rhs;
-  T d = T(1);
+  T xv[HPCGX_STENCIL];
 #pragma unroll
   for (int s = 0; s < HPCGX_STENCIL; ++s) {
-    const T v = to_arith(__ldg(A.vals + base + s * HPCGX_SLICE), T());
+    if (s == HPCGX_DIAG_SLOT) continue;
+    if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
+    xv[s] = (ZERO && col[s] == id.row) ? T(0) : x[col[s]];
+  }
+  T sum = rhs;
+  const T d = to_arith(val[HPCGX_DIAG_SLOT], T());
+#pragma unroll
+  for (int s = 0; s < HPCGX_STENCIL; ++s) {
     if (s == HPCGX_DIAG_SLOT) {
-      d = v;
-      if (!ZERO) sum = rn_sub(sum, rn_mul(v, xi));
+      if (!ZERO) sum = rn_sub(sum, rn_mul(d, xi));
       continue;
     }
-    if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
-    const int32_t col = __ldg(A.cols + base + s * HPCGX_SLICE);
-    sum = rn_sub(sum, rn_mul(v, x[col]));
+    if (ZERO && (((c ^ slot_mask(s)) > c) || col[s] == id.row)) continue;
+    sum = rn_sub(sum, rn_mul(to_arith(val[s], T()), xv[s]));
   }
   if (!ZERO) sum = rn_add(sum, rn_mul(xi, d));
   const T xn = rn_div(sum, d);
@@ -267,31 +288,32 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   if (RES) {
     T ax = T(0);
 #pragma unroll
-    for (int s = 0; s < HPCGX_STENCIL; ++s) {
-      const T v = to_arith(__ldg(A.vals + base + s * HPCGX_SLICE), T());
-      const T xv = (s == HPCGX_DIAG_SLOT) ? xn : x[__ldg(A.cols + base + s * HPCGX_SLICE)];
-      ax = rn_add(ax, rn_mul(v, xv));
-    }
+    for (int s = 0; s < HPCGX_STENCIL; ++s)
+      ax = rn_add(ax, rn_mul(to_arith(val[s], T()), s == HPCGX_DIAG_SLOT ? xn : xv[s]));
     rc[crow] = rn_sub(rhs, ax);
   }
 }
 
-// A half sweep over one class: colours 2q then 2q+1 (forward) or 2q+1 then 2q
-// (backward).  MODE bits: GS_ZERO_GUESS for the whole launch; GS_PROLONG and
-// GS_RESTRICT act on colour 0 only.
-template <int MODE, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads)
-k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, int backward, const RT *__restrict__ r, T *x,
+// A half sweep over one class: colours 2q then 2q+1 (forward, DIR = 0) or
+// 2q+1 then 2q (backward, DIR = 1).  MODE bits: GS_ZERO_GUESS for the whole
+// launch; GS_PROLONG and GS_RESTRICT act on colour 0 only.  QS >= 0 fixes the
+// class at compile time, which lets the zero-guess sweep drop the loads of the
+// skipped slots statically.
+template <int MODE, int DIR, int QS, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads, 2)
+k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
            const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
   if (done && *done) return;
   constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0;
   constexpr bool PRO = (MODE & GS_PROLONG) != 0;
   constexpr bool RES = (MODE & GS_RESTRICT) != 0;
+  const int q = QS >= 0 ? QS : C.q;
   const int j0 = blockIdx.x * lpb;
   const int j1 = min(j0 + lpb, C.lines);
+#pragma unroll
   for (int half = 0; half < 2; ++half) {
-    const int px = backward ? 1 - half : half;
-    const int c = px + 2 * C.q;
+    const int px = DIR ? 1 - half : half;
+    const int c = px + 2 * q;
     const int cnt = (j1 - j0) * C.len[px];
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
       const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
@@ -883,22 +905,29 @@ int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *
   const dim3 g(L.blocks[q]), b(L.threads[q]);
   const int lpb = L.lines_per_block[q];
   const ClassInfo &C = L.cls[q];
-  switch (mode) {
-    case GS_PLAIN:
-      k_gs_class<GS_PLAIN><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
-      return 1;
-    case GS_ZERO_GUESS:
-      k_gs_class<GS_ZERO_GUESS><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
-      return 1;
-    case GS_RESTRICT:
-      k_gs_class<GS_RESTRICT><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
-      return 1;
-    case GS_PROLONG:
-      k_gs_class<GS_PROLONG><<<g, b, 0, s>>>(A, C, lpb, backward, r, x, xc, rc, done);
-      return 1;
-    default:
-      return 0;
+  if (mode == GS_ZERO_GUESS && !backward) {
+    switch (q) {
+      case 0: k_gs_class<GS_ZERO_GUESS, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      case 1: k_gs_class<GS_ZERO_GUESS, 0, 1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      case 2: k_gs_class<GS_ZERO_GUESS, 0, 2><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      default: k_gs_class<GS_ZERO_GUESS, 0, 3><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+    }
+    return 1;
   }
+  if (mode == GS_RESTRICT && backward && q == 0) {
+    k_gs_class<GS_RESTRICT, 1, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    return 1;
+  }
+  if (mode == GS_PROLONG && !backward && q == 0) {
+    k_gs_class<GS_PROLONG, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    return 1;
+  }
+  if (mode != GS_PLAIN) return 0;
+  if (backward)
+    k_gs_class<GS_PLAIN, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+  else
+    k_gs_class<GS_PLAIN, 0, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+  return 1;
 }
 
 template int launch_gs_class<double, double>(const LevelDev &, int, int, int, const double *,

@@ -98,8 +98,11 @@ def test_mg_bitexact_colour_order(grid, oracle):
     _, r, _ = seeded(oracle, L[0].nrow)
     z = host(P.mg(cuda(r)))
     assert (z == oracle.mg(L, r, coloured=True)).all()
-    # calling again must not depend on leftovers in the work vectors
+    # calling again must not depend on leftovers in the work vectors, and the
+    # output is written, never read (ComputeMG zeroes x first)
     assert (host(P.mg(cuda(r))) == z).all()
+    junk = torch.full((L[0].nrow,), float("nan"), dtype=torch.float64, device="cuda")
+    assert (host(P.mg(cuda(r), junk)) == z).all()
 
 
 def test_against_reference_golden(oracle):
@@ -234,7 +237,8 @@ def test_mixed_bitexact(grid, oracle):
         xd = cuda(x32)
         P.symgs_mixed(cuda(rr), xd, level=l)
         assert (host(xd) == oracle.symgs32(lev, rr, x32)).all()
-    assert (host(P.mg_mixed(cuda(r))) == oracle.mg32(L, r)).all()
+    junk = torch.full((L[0].nrow,), float("nan"), dtype=torch.float32, device="cuda")
+    assert (host(P.mg_mixed(cuda(r), junk)) == oracle.mg32(L, r)).all()
 
 
 def test_mixed_cg(grid, oracle):
