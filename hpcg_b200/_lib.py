@@ -46,6 +46,7 @@ SIGNATURES = {
     "hpcgx_dot": (_I, [_P, _I64, _P, _P, _DP]),
     "hpcgx_waxpby": (_I, [_P, _I64, _D, _P, _D, _P, _P]),
     "hpcgx_residual": (_I, [_P, _I64, _P, _P, _DP]),
+    "hpcgx_dot_noalloc": (_I, [_I64, _P, _P, _P, _P]),
     "hpcgx_spmv_mixed": (_I, [_P, _I, _P, _P]),
     "hpcgx_symgs_mixed": (_I, [_P, _I, _P, _P, _P]),
     "hpcgx_mg_mixed": (_I, [_P, _P, _P]),

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libhpcgx.so")
-SOURCES = ["kernels.cu", "problem.cu"]
+SOURCES = ["kernels.cu", "problem.cu", "noalloc.cu"]
 HEADERS = ["common.cuh", "kernels.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

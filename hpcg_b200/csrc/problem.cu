@@ -72,6 +72,11 @@ struct Probe {
 
 }  // namespace
 
+namespace hpcgx {
+// Records an error message for hpcgx_last_error() from other translation units.
+int set_error(int code, const char *msg) { return fail(code, msg); }
+}  // namespace hpcgx
+
 struct hpcgx_problem {
   int device = 0;
   int nlev = 0;

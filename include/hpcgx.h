@@ -122,6 +122,25 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
                       float *x);
 int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x);
 
+/* Dot product that allocates nothing (no counterpart in the reference).  For
+ * callers that may not allocate device memory -- code living inside another
+ * framework's memory pool, or latency-critical loops in which cudaMalloc /
+ * cudaFree would stall or synchronise the device.  It needs no problem
+ * handle: the per-block partial sums live in a fixed 256 KiB array inside the
+ * library (present on every GPU that loads the library, until exit).
+ *   - n must not exceed HPCGX_DOT_NOALLOC_MAX_N (67,108,864 elements);
+ *     larger n returns HPCGX_EINVAL (use hpcgx_dot);
+ *   - x, y: device vectors of the current device; result: one device double;
+ *   - runs asynchronously on `stream` (NULL: the legacy default stream);
+ *   - the first call on a device looks up the array's device address; make
+ *     that first call before any stream capture on that device;
+ *   - every call shares the one array, so calls that overlap on the GPU (on
+ *     different streams, or from several host threads) race and must not be
+ *     issued concurrently. */
+#define HPCGX_DOT_NOALLOC_MAX_N 67108864LL
+int hpcgx_dot_noalloc(int64_t n, const double *x, const double *y, double *result,
+                      void *stream);
+
 /* ---- solvers ------------------------------------------------------------ */
 
 /* CG (src/CG.hpp:22-24) on device vectors: b read, x initial guess in and
