@@ -47,6 +47,11 @@ SIGNATURES = {
     "hpcgx_waxpby": (_I, [_P, _I64, _D, _P, _D, _P, _P]),
     "hpcgx_residual": (_I, [_P, _I64, _P, _P, _DP]),
     "hpcgx_dot_noalloc": (_I, [_I64, _P, _P, _P, _P]),
+    "hpcgx_spmv_host": (_I, [_P, _I, _P, _P]),
+    "hpcgx_symgs_host": (_I, [_P, _I, _P, _P]),
+    "hpcgx_mg_host": (_I, [_P, _P, _P]),
+    "hpcgx_dot_host": (_I, [_P, _I64, _P, _P, _DP]),
+    "hpcgx_waxpby_host": (_I, [_P, _I64, _D, _P, _D, _P, _P]),
     "hpcgx_spmv_mixed": (_I, [_P, _I, _P, _P]),
     "hpcgx_symgs_mixed": (_I, [_P, _I, _P, _P, _P]),
     "hpcgx_mg_mixed": (_I, [_P, _P, _P]),
@@ -67,6 +72,7 @@ HPCGX_OK = 0
 ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ESTATE", 4: "ENONFINITE", 5: "ELAYOUT", 6: "ENOMEM"}
 GEN_HPCG, GEN_VARCOEF = 0, 1
 PROBE_NONE, PROBE_GS_FINE, PROBE_SPMV_FINE = 0, 1, 2
+CG_PLAIN, CG_MG, CG_MIXED = 0, 1, 2
 
 
 class HPCGXError(RuntimeError):

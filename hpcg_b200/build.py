@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out)
         if verbose and out:
             print(out)
-    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-Xlinker", "-soname=libhpcgx.so", "-o", LIB, *objs]
     out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("nvcc link failed:\n" + out.stdout + out.stderr)

@@ -90,6 +90,7 @@ struct hpcgx_problem {
   double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
   float *z32 = nullptr;
   double *tmp = nullptr;      // staging for host diagonals
+  double *stage[3] = {};      // staging of the host-buffer operators (allocated on first use)
   double *result = nullptr;   // device scalars of standalone reductions
   CgState *st = nullptr;
   Reduce red;
@@ -223,6 +224,21 @@ struct hpcgx_problem {
   int symgs(int l, const RT *r, T *x) {
     for (int q = 0; q < 4; ++q) note(launch_gs_class<T, RT>(L[l], q, 0, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
     for (int q = 3; q >= 0; --q) note(launch_gs_class<T, RT>(L[l], q, 1, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
+    return HPCGX_OK;
+  }
+
+  int staging() {
+    for (double *&ptr : stage)
+      if (!ptr) TRY(alloc((void **)&ptr, L[0].n * sizeof(double)));
+    return HPCGX_OK;
+  }
+  int up(double *dst, const double *src, int64_t n) {
+    CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    return HPCGX_OK;
+  }
+  int down(double *dst, const double *src, int64_t n) {
+    CK(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
     return HPCGX_OK;
   }
 
@@ -422,6 +438,7 @@ hpcgx_problem::~hpcgx_problem() {
     cudaFree(L[l].r32);
     cudaFree(L[l].x32);
   }
+  for (double *ptr : stage) cudaFree(ptr);
   for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)z, (void *)p, (void *)Ap,
                     (void *)z32, (void *)tmp, (void *)result, (void *)st,
                     (void *)red.partials, (void *)red.counter})
@@ -813,17 +830,74 @@ int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter, d
   return p->cg(G_MIXED, b, x, max_iter, tolerance, niters, normr, normr0, times);
 }
 
-int hpcgx_cg_host(hpcgx_problem *p, int mixed, const double *b_host, double *x_host, int max_iter,
+int hpcgx_cg_host(hpcgx_problem *p, int mode, const double *b_host, double *x_host, int max_iter,
                   double tolerance, int *niters, double *normr, double *normr0, double *times) {
   HANDLE(p);
   const int64_t n = p->L[0].n;
+  int kind;
+  switch (mode) {
+    case HPCGX_CG_PLAIN: kind = G_FP64_NOPREC; break;
+    case HPCGX_CG_MG: kind = G_FP64_PREC; break;
+    case HPCGX_CG_MIXED: kind = G_MIXED; break;
+    default: return fail(HPCGX_EINVAL, "unknown CG mode");
+  }
   CK(cudaMemcpyAsync(p->b, b_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
   CK(cudaMemcpyAsync(p->x, x_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-  TRY(p->cg(mixed ? G_MIXED : G_FP64_PREC, p->b, p->x, max_iter, tolerance, niters, normr, normr0,
-            times));
+  TRY(p->cg(kind, p->b, p->x, max_iter, tolerance, niters, normr, normr0, times));
   CK(cudaMemcpyAsync(x_host, p->x, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   return HPCGX_OK;
+}
+
+int hpcgx_spmv_host(hpcgx_problem *p, int level, const double *x, double *y) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  TRY(p->staging());
+  const int64_t n = p->L[level].n;
+  TRY(p->up(p->stage[0], x, n));
+  TRY(hpcgx_spmv(p, level, p->stage[0], p->stage[1]));
+  return p->down(y, p->stage[1], n);
+}
+
+int hpcgx_symgs_host(hpcgx_problem *p, int level, const double *r, double *x) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  TRY(p->staging());
+  const int64_t n = p->L[level].n;
+  TRY(p->up(p->stage[0], r, n));
+  TRY(p->up(p->stage[1], x, n));
+  TRY(hpcgx_symgs(p, level, p->stage[0], p->stage[1]));
+  return p->down(x, p->stage[1], n);
+}
+
+int hpcgx_mg_host(hpcgx_problem *p, const double *r, double *x) {
+  HANDLE(p);
+  TRY(p->staging());
+  const int64_t n = p->L[0].n;
+  TRY(p->up(p->stage[0], r, n));
+  TRY(hpcgx_mg(p, p->stage[0], p->stage[1]));
+  return p->down(x, p->stage[1], n);
+}
+
+int hpcgx_dot_host(hpcgx_problem *p, int64_t n, const double *x, const double *y,
+                   double *result) {
+  HANDLE(p);
+  if (n < 0 || n > p->L[0].n) return fail(HPCGX_EINVAL, "bad dot length");
+  TRY(p->staging());
+  TRY(p->up(p->stage[0], x, n));
+  if (y != x) TRY(p->up(p->stage[1], y, n));
+  return hpcgx_dot(p, n, p->stage[0], y == x ? p->stage[0] : p->stage[1], result);
+}
+
+int hpcgx_waxpby_host(hpcgx_problem *p, int64_t n, double alpha, const double *x, double beta,
+                      const double *y, double *w) {
+  HANDLE(p);
+  if (n < 0 || n > p->L[0].n) return fail(HPCGX_EINVAL, "bad waxpby length");
+  TRY(p->staging());
+  TRY(p->up(p->stage[0], x, n));
+  TRY(p->up(p->stage[1], y, n));
+  TRY(hpcgx_waxpby(p, n, alpha, p->stage[0], beta, p->stage[1], p->stage[2]));
+  return p->down(w, p->stage[2], n);
 }
 
 int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, double *grad) {

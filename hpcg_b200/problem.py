@@ -216,12 +216,13 @@ class Problem:
                                    C.byref(it), C.byref(nr), C.byref(nr0), tp))
         return it.value, nr.value, nr0.value
 
-    def cg_host(self, b_host, x_host, max_iter, tol, mixed=False, times=None):
+    def cg_host(self, b_host, x_host, max_iter, tol, mixed=False, precond=True, times=None):
         """Solve from host buffers (numpy or pinned CPU tensors); x_host updated."""
         self._pre()
         it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
         tp = _ptr(times) if times is not None else None
-        check(lib().hpcgx_cg_host(self.h, int(mixed), _ptr(b_host), _ptr(x_host), int(max_iter),
+        mode = _lib.CG_MIXED if mixed else (_lib.CG_MG if precond else _lib.CG_PLAIN)
+        check(lib().hpcgx_cg_host(self.h, mode, _ptr(b_host), _ptr(x_host), int(max_iter),
                                   float(tol), C.byref(it), C.byref(nr), C.byref(nr0), tp))
         return it.value, nr.value, nr0.value
 

@@ -114,6 +114,18 @@ int hpcgx_waxpby(hpcgx_problem *p, int64_t n, double alpha, const double *x, dou
 int hpcgx_residual(hpcgx_problem *p, int64_t n, const double *v1, const double *v2,
                    double *result_host);
 
+/* Host-buffer forms of the operators above, for callers that hold host
+ * vectors (the reference's Vector::values): the inputs are copied to device
+ * staging buffers of the problem, the operator runs, and the outputs are
+ * copied back.  These serve the drop-in operator files in hpcg_b200/dropin. */
+int hpcgx_spmv_host(hpcgx_problem *p, int level, const double *x_host, double *y_host);
+int hpcgx_symgs_host(hpcgx_problem *p, int level, const double *r_host, double *x_host);
+int hpcgx_mg_host(hpcgx_problem *p, const double *r_host, double *x_host);
+int hpcgx_dot_host(hpcgx_problem *p, int64_t n, const double *x_host, const double *y_host,
+                   double *result_host);
+int hpcgx_waxpby_host(hpcgx_problem *p, int64_t n, double alpha, const double *x_host,
+                      double beta, const double *y_host, double *w_host);
+
 /* Mixed-precision operators (BF16 values, FP32 vectors; no reference
  * counterpart): y = A x, one symmetric sweep with an FP64 (r64) or FP32 (r32)
  * right-hand side, and the FP32 V-cycle of an FP64 residual. */
@@ -156,8 +168,13 @@ int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter,
                    double tolerance, int *niters, double *normr, double *normr0,
                    double *times);
 /* The same solves from host buffers (pinned memory gives full copy speed):
- * b_host and x_host are copied to the device, solved, and x copied back. */
-int hpcgx_cg_host(hpcgx_problem *p, int mixed, const double *b_host, double *x_host,
+ * b_host and x_host are copied to the device, solved, and x copied back.
+ * mode: HPCGX_CG_PLAIN (unpreconditioned), HPCGX_CG_MG (FP64 MG-PCG, the
+ * reference's CG), HPCGX_CG_MIXED (flexible CG, FP32/BF16 V-cycle). */
+#define HPCGX_CG_PLAIN 0
+#define HPCGX_CG_MG 1
+#define HPCGX_CG_MIXED 2
+int hpcgx_cg_host(hpcgx_problem *p, int mode, const double *b_host, double *x_host,
                   int max_iter, double tolerance, int *niters, double *normr,
                   double *normr0, double *times);
 
