@@ -6,5 +6,6 @@ torch CUDA tensors; ``solve`` is the differentiable solve.
 """
 from ._lib import HPCGXError, lib  # noqa: F401
 from .problem import Problem  # noqa: F401
+from .autograd import solve, symmetric_direction, varcoef_problem  # noqa: F401
 
-__all__ = ["Problem", "HPCGXError", "lib"]
+__all__ = ["Problem", "HPCGXError", "lib", "solve", "varcoef_problem", "symmetric_direction"]

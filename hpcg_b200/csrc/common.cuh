@@ -7,9 +7,13 @@
 //     keep natural order, so each colour is a list of x-lines (fixed iy, iz)
 //     holding every other point;
 //   * every colour starts on a 32-row boundary; rows are grouped in slices of
-//     32 and a slice stores its 27 slots column-major: element (row k, slot s)
-//     lives at (k/32)*27*32 + s*32 + k%32, so a warp reading one slot of 32
-//     consecutive rows issues one 256-byte (FP64) load;
+//     32 rows x 27 slots.  Inside a slice the slots are grouped per stencil
+//     z-plane (9 slots each) and, inside a plane, interleaved across the 32
+//     rows in short vectors: FP64 values in pairs of slots (one 16-byte load
+//     per row and pair), int32 columns and BF16 values in quads (one 16- or
+//     8-byte load), plus one single slot per plane.  A warp's load of one
+//     group for its 32 rows is one contiguous 512 / 256-byte segment, and a
+//     row needs 15 value loads and 9 column loads instead of 27 + 27;
 //   * slot s is the stencil offset (dz+1)*9 + (dy+1)*3 + (dx+1); slot 13 is the
 //     diagonal.  Absent neighbours (boundary rows) hold value 0 and column =
 //     the row itself.  Present entries therefore appear in exactly the
@@ -50,8 +54,25 @@ struct LevelMat {
   int64_t n;
 };
 
-__host__ __device__ inline int64_t ell_index(int64_t k, int s) {
-  return (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (int64_t)s * HPCGX_SLICE + (k & 31);
+// Elements of one 32-row slice and of one z-plane inside it.
+constexpr int kSliceElems = HPCGX_STENCIL * HPCGX_SLICE;  // 864
+constexpr int kPlaneElems = 9 * HPCGX_SLICE;              // 288
+
+// Index of (storage row k, slot s) in the FP64 value array: per plane, slots
+// r = 0..7 in interleaved pairs, slot r = 8 alone.
+__host__ __device__ inline int64_t vidx(int64_t k, int s) {
+  const int p = s / 9, r = s - 9 * p;
+  const int64_t base = (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+  return r < 8 ? base + (r >> 1) * 64 + lane * 2 + (r & 1) : base + 256 + lane;
+}
+// Index of (storage row k, slot s) in the column and BF16 value arrays: per
+// plane, slots r = 0..7 in interleaved quads, slot r = 8 alone.
+__host__ __device__ inline int64_t cidx(int64_t k, int s) {
+  const int p = s / 9, r = s - 9 * p;
+  const int64_t base = (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+  return r < 8 ? base + (r >> 2) * 128 + lane * 4 + (r & 3) : base + 256 + lane;
 }
 
 // Colour of the neighbour in slot s of a row of colour c.

@@ -181,6 +181,69 @@ __device__ __forceinline__ RowId row_of(const ClassInfo &C, int nx, int ny, int 
   return r;
 }
 
+// ---------------------------------------------------------------- row loads
+
+// Vector loads of one stencil z-plane (9 slots) of storage row k; a group is
+// loaded only if need(s) holds for one of its slots (need folds to a
+// constant in every kernel, so skipped groups cost nothing).
+template <class NEED>
+__device__ __forceinline__ void load_plane(const double *__restrict__ vals, int64_t k, int p,
+                                           NEED need, double *v) {
+  const double *q = vals + (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    if (need(9 * p + 2 * j) || need(9 * p + 2 * j + 1)) {
+      const double2 t = __ldg(reinterpret_cast<const double2 *>(q + j * 64 + lane * 2));
+      v[2 * j] = t.x;
+      v[2 * j + 1] = t.y;
+    }
+  }
+  if (need(9 * p + 8)) v[8] = __ldg(q + 256 + lane);
+}
+
+template <class NEED>
+__device__ __forceinline__ void load_plane(const uint16_t *__restrict__ vals, int64_t k, int p,
+                                           NEED need, uint16_t *v) {
+  const uint16_t *q = vals + (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (need(9 * p + 4 * j) || need(9 * p + 4 * j + 1) || need(9 * p + 4 * j + 2) ||
+        need(9 * p + 4 * j + 3)) {
+      const uint2 t = __ldg(reinterpret_cast<const uint2 *>(q + j * 128 + lane * 4));
+      v[4 * j] = (uint16_t)(t.x & 0xffffu);
+      v[4 * j + 1] = (uint16_t)(t.x >> 16);
+      v[4 * j + 2] = (uint16_t)(t.y & 0xffffu);
+      v[4 * j + 3] = (uint16_t)(t.y >> 16);
+    }
+  }
+  if (need(9 * p + 8)) v[8] = __ldg(q + 256 + lane);
+}
+
+template <class NEED>
+__device__ __forceinline__ void load_plane(const int32_t *__restrict__ cols, int64_t k, int p,
+                                           NEED need, int32_t *c) {
+  const int32_t *q = cols + (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (need(9 * p + 4 * j) || need(9 * p + 4 * j + 1) || need(9 * p + 4 * j + 2) ||
+        need(9 * p + 4 * j + 3)) {
+      const int4 t = __ldg(reinterpret_cast<const int4 *>(q + j * 128 + lane * 4));
+      c[4 * j] = t.x;
+      c[4 * j + 1] = t.y;
+      c[4 * j + 2] = t.z;
+      c[4 * j + 3] = t.w;
+    }
+  }
+  if (need(9 * p + 8)) c[8] = __ldg(q + 256 + lane);
+}
+
+struct NeedAll {
+  __device__ constexpr bool operator()(int) const { return true; }
+};
+
 // ---------------------------------------------------------------- SpMV
 
 // y = A x, rows summed left to right over the slots as ComputeSPMV_ref does
@@ -203,13 +266,12 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
     const int cnt = (j1 - j0) * C.len[px];
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
       const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
-      const int64_t base = (id.k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (id.k & 31);
       int32_t col[HPCGX_STENCIL];
       VT val[HPCGX_STENCIL];
 #pragma unroll
-      for (int s = 0; s < HPCGX_STENCIL; ++s) {
-        col[s] = __ldg(A.cols + base + s * HPCGX_SLICE);
-        val[s] = __ldg(A.vals + base + s * HPCGX_SLICE);
+      for (int p = 0; p < 3; ++p) {
+        load_plane(A.cols, id.k, p, NeedAll(), col + 9 * p);
+        load_plane(A.vals, id.k, p, NeedAll(), val + 9 * p);
       }
       T xv[HPCGX_STENCIL];
 #pragma unroll
@@ -247,14 +309,14 @@ template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
 __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, int c,
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
                                        T *__restrict__ rc) {
-  const int64_t base = (id.k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (id.k & 31);
   int32_t col[HPCGX_STENCIL];
   VT val[HPCGX_STENCIL];
+  // slots whose neighbour is read: all, or (zero guess) the lower colours
+  auto need = [c](int s) { return !ZERO || s == HPCGX_DIAG_SLOT || ((c ^ slot_mask(s)) < c); };
 #pragma unroll
-  for (int s = 0; s < HPCGX_STENCIL; ++s) {
-    if (ZERO && s != HPCGX_DIAG_SLOT && ((c ^ slot_mask(s)) > c)) continue;
-    val[s] = __ldg(A.vals + base + s * HPCGX_SLICE);
-    if (s != HPCGX_DIAG_SLOT) col[s] = __ldg(A.cols + base + s * HPCGX_SLICE);
+  for (int p = 0; p < 3; ++p) {
+    load_plane(A.vals, id.k, p, need, val + 9 * p);
+    load_plane(A.cols, id.k, p, need, col + 9 * p);
   }
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
@@ -555,7 +617,6 @@ __global__ void k_generate_hpcg(Geo g, int64_t storage_rows, double *vals, int32
     int64_t row;
     int ix, iy, iz;
     const bool real = storage_to_natural(g, k, row, ix, iy, iz);
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
       int64_t col = 0;
       double v = 0.0;
@@ -565,8 +626,8 @@ __global__ void k_generate_hpcg(Geo g, int64_t storage_rows, double *vals, int32
         else
           col = row;
       }
-      vals[base + s * HPCGX_SLICE] = v;
-      cols[base + s * HPCGX_SLICE] = (int32_t)col;
+      vals[vidx(k, s)] = v;
+      cols[cidx(k, s)] = (int32_t)col;
     }
   }
 }
@@ -581,7 +642,6 @@ __global__ void k_generate_varcoef(Geo g, int64_t storage_rows, int level, int n
     int64_t row;
     int ix, iy, iz;
     const bool real = storage_to_natural(g, k, row, ix, iy, iz);
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
     double dsum = 0.0;
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
       int64_t col = 0;
@@ -604,10 +664,10 @@ __global__ void k_generate_varcoef(Geo g, int64_t storage_rows, int level, int n
           col = row;
         }
       }
-      vals[base + s * HPCGX_SLICE] = v;
-      cols[base + s * HPCGX_SLICE] = (int32_t)col;
+      vals[vidx(k, s)] = v;
+      cols[cidx(k, s)] = (int32_t)col;
     }
-    if (real) vals[base + HPCGX_DIAG_SLOT * HPCGX_SLICE] = dsum + 2.0;
+    if (real) vals[vidx(k, HPCGX_DIAG_SLOT)] = dsum + 2.0;
   }
 }
 
@@ -621,7 +681,6 @@ __global__ void k_coarsen_varcoef(Geo gf, Geo gc, int64_t storage_rows_c,
     int64_t row;
     int ix, iy, iz;
     if (!storage_to_natural(gc, k, row, ix, iy, iz)) continue;
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
     double dsum = 0.0;
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
       if (s == HPCGX_DIAG_SLOT) continue;
@@ -636,19 +695,22 @@ __global__ void k_coarsen_varcoef(Geo gf, Geo gc, int64_t storage_rows_c,
       }
       const int64_t frow = ((int64_t)(2 * lz) * gf.ny + 2 * ly) * gf.nx + 2 * lx;
       const int64_t fk = natural_to_storage(gf, frow);
-      const double v = fvals[(fk >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (int64_t)sl * HPCGX_SLICE +
-                             (fk & 31)];
-      cvals[base + s * HPCGX_SLICE] = v;
+      const double v = fvals[vidx(fk, sl)];
+      cvals[vidx(k, s)] = v;
       dsum += fabs(v);
     }
-    cvals[base + HPCGX_DIAG_SLOT * HPCGX_SLICE] = dsum + 2.0;
+    cvals[vidx(k, HPCGX_DIAG_SLOT)] = dsum + 2.0;
   }
 }
 
+// BF16 copy of the FP64 values (the two arrays group slots differently).
 __global__ void k_to_bf16(int64_t m, const double *__restrict__ v, uint16_t *h) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
-       i += (int64_t)gridDim.x * blockDim.x)
-    h[i] = bf16_from_double(v[i]);
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = i / HPCGX_STENCIL;
+    const int s = (int)(i - k * HPCGX_STENCIL);
+    h[cidx(k, s)] = bf16_from_double(v[vidx(k, s)]);
+  }
 }
 
 // Values in natural row order, 27 stencil slots per row -> device layout.
@@ -659,11 +721,10 @@ __global__ void k_set_values(Geo g, int64_t n, const double *__restrict__ in, do
     const int64_t k = natural_to_storage(g, row);
     const int ix = (int)(row % g.nx), iy = (int)((row / g.nx) % g.ny),
               iz = (int)(row / ((int64_t)g.nx * g.ny));
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
       int64_t col;
       const bool has = neighbour(g, ix, iy, iz, s, row, col);
-      vals[base + s * HPCGX_SLICE] = has ? in[row * HPCGX_STENCIL + s] : 0.0;
+      vals[vidx(k, s)] = has ? in[row * HPCGX_STENCIL + s] : 0.0;
     }
   }
 }
@@ -673,10 +734,9 @@ __global__ void k_get_values(Geo g, int64_t n, const double *__restrict__ vals,
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
        row += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = natural_to_storage(g, row);
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
-      if (out) out[row * HPCGX_STENCIL + s] = vals[base + s * HPCGX_SLICE];
-      if (cout) cout[row * HPCGX_STENCIL + s] = cols[base + s * HPCGX_SLICE];
+      if (out) out[row * HPCGX_STENCIL + s] = vals[vidx(k, s)];
+      if (cout) cout[row * HPCGX_STENCIL + s] = cols[cidx(k, s)];
     }
   }
 }
@@ -685,7 +745,7 @@ __global__ void k_set_diagonal(Geo g, int64_t n, const double *__restrict__ d, d
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
        row += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = natural_to_storage(g, row);
-    vals[(k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + HPCGX_DIAG_SLOT * HPCGX_SLICE + (k & 31)] = d[row];
+    vals[vidx(k, HPCGX_DIAG_SLOT)] = d[row];
   }
 }
 
@@ -693,7 +753,7 @@ __global__ void k_get_diagonal(Geo g, int64_t n, const double *__restrict__ vals
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
        row += (int64_t)gridDim.x * blockDim.x) {
     const int64_t k = natural_to_storage(g, row);
-    d[row] = vals[(k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + HPCGX_DIAG_SLOT * HPCGX_SLICE + (k & 31)];
+    d[row] = vals[vidx(k, HPCGX_DIAG_SLOT)];
   }
 }
 
@@ -707,13 +767,11 @@ __global__ void k_adjoint_grad(Geo g, int64_t n, const int32_t *__restrict__ col
     const int64_t k = natural_to_storage(g, row);
     const int ix = (int)(row % g.nx), iy = (int)((row / g.nx) % g.ny),
               iz = (int)(row / ((int64_t)g.nx * g.ny));
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
     const double li = lambda[row];
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
       int64_t col;
       const bool has = neighbour(g, ix, iy, iz, s, row, col);
-      grad[row * HPCGX_STENCIL + s] =
-          has ? -(li * x[__ldg(cols + base + s * HPCGX_SLICE)]) : 0.0;
+      grad[row * HPCGX_STENCIL + s] = has ? -(li * x[__ldg(cols + cidx(k, s))]) : 0.0;
     }
   }
 }

@@ -474,8 +474,7 @@ int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
     const int ix = (int)(row % A.nx), iy = (int)((row / A.nx) % A.ny),
               iz = (int)(row / ((int64_t)A.nx * A.ny));
     const int64_t k = storage_row_host(A, row);
-    const int64_t base = (k >> 5) * (HPCGX_STENCIL * HPCGX_SLICE) + (k & 31);
-    for (int s = 0; s < HPCGX_STENCIL; ++s) cols[base + s * HPCGX_SLICE] = (int32_t)row;
+    for (int s = 0; s < HPCGX_STENCIL; ++s) cols[cidx(k, s)] = (int32_t)row;
     const int nz = nnz_of(row);
     if (nz < 1 || nz > HPCGX_STENCIL)
       return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + " has " + std::to_string(nz) +
@@ -499,8 +498,8 @@ int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
                                        ": entries not in stencil order");
       last = s;
       diag |= (s == HPCGX_DIAG_SLOT);
-      vals[base + s * HPCGX_SLICE] = v;
-      cols[base + s * HPCGX_SLICE] = col;
+      vals[vidx(k, s)] = v;
+      cols[cidx(k, s)] = col;
     }
     if (!diag) return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + " has no diagonal");
   }

@@ -47,6 +47,7 @@ class Problem:
         self.h = h
         self.stream = torch.cuda.Stream(device=self.device)
         check(lib().hpcgx_set_stream(self.h, C.c_void_p(self.stream.cuda_stream)))
+        self.values_version = 0     # bumped whenever matrix values change
 
     # ----------------------------------------------------------- lifetime
     def close(self):
@@ -86,6 +87,7 @@ class Problem:
     def generate(self, kind="hpcg", seed=0, sigma=0.0):
         code = {"hpcg": _lib.GEN_HPCG, "varcoef": _lib.GEN_VARCOEF}[kind]
         check(lib().hpcgx_generate(self.h, code, seed, float(sigma)))
+        self.values_version += 1
         return self
 
     def load_level(self, level, nnz, cols, vals):
@@ -94,6 +96,7 @@ class Problem:
         cols = np.ascontiguousarray(cols, np.int32)
         vals = np.ascontiguousarray(vals, np.float64)
         check(lib().hpcgx_load_level(self.h, level, _ptr(nnz), _ptr(cols), _ptr(vals)))
+        self.values_version += 1
 
     def check_f2c(self, level, f2c):
         f2c = np.ascontiguousarray(f2c, np.int32)
@@ -105,6 +108,7 @@ class Problem:
     def set_diagonal(self, level, diag):
         d = np.ascontiguousarray(diag, np.float64)
         check(lib().hpcgx_set_diagonal_host(self.h, level, _ptr(d)))
+        self.values_version += 1
 
     def get_diagonal(self, level=0):
         d = np.zeros(self.rows(level))
@@ -115,6 +119,7 @@ class Problem:
         self._pre()
         v = vals27.contiguous()
         check(lib().hpcgx_set_values(self.h, level, _ptr(v), int(recoarsen)))
+        self.values_version += 1
 
     def get_values(self, level=0):
         self._pre()

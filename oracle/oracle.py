@@ -344,6 +344,7 @@ class RefProblem:
             lib.ref_export_level.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P]
             lib.ref_get_vectors.argtypes = [_P, _P, _P, _P]
             lib.ref_replace_diagonal.argtypes = [_P, C.c_int, _P]
+            lib.ref_set_level_values.argtypes = [_P, C.c_int, _P]
             for f in ("ref_spmv", "ref_symgs", "ref_symgs_permuted"):
                 getattr(lib, f).argtypes = [_P, C.c_int, _P, _P]
             lib.ref_mg.argtypes = [_P, _P, _P]
@@ -402,6 +403,9 @@ class RefProblem:
 
     def replace_diagonal(self, level, d):
         self.lib().ref_replace_diagonal(self.h, level, _ptr(np.ascontiguousarray(d)))
+
+    def set_level_values(self, level, vals):
+        self.lib().ref_set_level_values(self.h, level, _ptr(np.ascontiguousarray(vals)))
 
     def spmv(self, level, x):
         y = np.zeros(self.rows(level))

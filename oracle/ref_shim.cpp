@@ -190,6 +190,14 @@ void ref_get_vectors(void *h, double *b, double *x, double *xexact) {
   if (xexact) std::memcpy(xexact, p->xexact.values, sizeof(double) * n);
 }
 
+// Overwrites the values of one level (contiguous 27-slot layout, entries in
+// the reference's order); the pattern and the diagonal pointers stay.
+void ref_set_level_values(void *h, int level, const double *vals) {
+  SparseMatrix &A = *static_cast<RefProblem *>(h)->level[level];
+  for (local_int_t i = 0; i < A.localNumberOfRows; i++)
+    for (int j = 0; j < A.nonzerosInRow[i]; j++) A.matrixValues[i][j] = vals[(int64_t)i * 27 + j];
+}
+
 // ReplaceMatrixDiagonal (src/SparseMatrix.hpp:139-145) on one level.
 void ref_replace_diagonal(void *h, int level, const double *d) {
   SparseMatrix &A = *static_cast<RefProblem *>(h)->level[level];

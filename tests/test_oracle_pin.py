@@ -167,3 +167,24 @@ def test_varcoef_generator_properties(oracle):
             off = sum(abs(A[(i, int(lev.cols[i * 27 + j]))]) for j in range(lev.nnz[i])
                       if lev.cols[i * 27 + j] != i)
             assert abs(A[(i, i)] - (off + 2.0)) <= 1e-12 * A[(i, i)]
+
+
+def test_varcoef_cg_against_reference(oracle):
+    """CG_ref of the reference build on the variable-coefficient hierarchy
+    agrees with the oracle's CG (both natural order)."""
+    from oracle.oracle import RefProblem
+    if not RefProblem.available():
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    dims = (16, 16, 16)
+    L, _, _, _ = oracle.hierarchy(*dims, varcoef=(2, 0.5))
+    n = L[0].nrow
+    ref = RefProblem(*dims)
+    for l, lev in enumerate(L):
+        ref.set_level_values(l, lev.vals)
+    b = oracle.uniform(3, n)
+    r = oracle.uniform(12, n)
+    assert (oracle.mg(L, r) == ref.mg(r)).all()
+    x1, k1, nr1, nr01 = oracle.cg(L, b, np.zeros(n), 500, 1e-12)
+    x2, k2, nr2, nr02, _ = ref.cg(b, np.zeros(n), 500, 1e-12)
+    assert k1 == k2 and np.abs(x1 - x2).max() < 1e-12
+    ref.close()
