@@ -188,6 +188,81 @@ def config(dims):
             "tolerance": TOL, "l2": "no flush: every step streams > 60 GB, far above the 126 MB L2"}
 
 
+def run_varcoef(args):
+    """Differentiable-solve workloads (no reference counterpart):
+    (3) 128^3, a_ij = -exp(0.5 z) (seed 2), b ~ U(0,1), x_target ~ N(0,1) (seed 3),
+        FP64 forward + adjoint to 1e-12, gradient vs central finite differences on 16
+        edge-symmetric directions (seed 4);
+    (4) 512x512x256, log-normal sigma = 1 (seed 5), b, x_target seed 6: mixed forward +
+        adjoint to 1e-10, wall time, gradient error vs the FP64 adjoint."""
+    import torch
+    from hpcg_b200 import solve, symmetric_direction, varcoef_problem
+    torch.cuda.set_device(0)
+    out = {"workload": "varcoef", "unit": "s"}
+
+    def loss(x, xt):
+        return 0.5 * torch.sum((x - xt) ** 2)
+
+    # ---- config 3: FD check
+    g3 = args.grid3
+    P, vals = varcoef_problem(g3, g3, g3, seed=2, sigma=0.5)
+    n = P.rows()
+    b = P.fill_uniform(3, 0.0, 1.0)
+    xt = P.fill_normal(3, offset=n)
+    v = vals.clone().requires_grad_(True)
+    bb = b.clone().requires_grad_(True)
+    x = solve(v, bb, P, tol=1e-12)
+    loss(x, xt).backward()
+    xs = x.detach()
+    gen = torch.Generator(device="cuda").manual_seed(4)
+    errs = []
+    for _ in range(16):
+        Dv = symmetric_direction(P, gen) * vals.abs()
+        Db = torch.randn(n, dtype=torch.float64, device="cuda", generator=gen)
+        h, dl = 1e-5, []
+        for sgn in (1.0, -1.0):
+            P.set_values((vals + sgn * h * Dv).reshape(-1), level=0, recoarsen=True)
+            xp = xs.clone()
+            P.cg(b + sgn * h * Db, xp, 2000, 1e-11)
+            d = xp - xs
+            dl.append(torch.sum(d * (xs - xt + 0.5 * d)).item())
+        fd = (dl[0] - dl[1]) / (2 * h)
+        an = (torch.sum(v.grad * Dv) + torch.sum(bb.grad * Db)).item()
+        errs.append(abs(fd - an) / abs(an))
+    out["config3"] = {"grid": [g3] * 3, "fd_rel_err_max": max(errs), "directions": 16,
+                      "tolerance": 1e-12}
+    P.close()
+    del P, vals, v, bb, x, xs
+    torch.cuda.empty_cache()
+    # ---- config 4: mixed forward + adjoint, timed; FP64 adjoint for the error
+    dims = tuple(args.grid4)
+    P, vals = varcoef_problem(*dims, seed=5, sigma=1.0)
+    P.build_mixed()
+    n = P.rows()
+    b = P.fill_uniform(6, 0.0, 1.0)
+    xt = P.fill_normal(6, offset=n)
+    res = {}
+    for mixed in (True, False, True):       # first pass warms up, the last one is timed
+        v = vals.clone().requires_grad_(True)
+        bb = b.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x = solve(v, bb, P, tol=1e-10, mixed=mixed)
+        loss(x, xt).backward()
+        torch.cuda.synchronize()
+        res[mixed] = (time.perf_counter() - t0, v.grad, bb.grad)
+        del v, bb, x
+    t_mixed, gv_m, gb_m = res[True]
+    t_fp64, gv_d, gb_d = res[False]
+    out["config4"] = {
+        "grid": list(dims), "fwd_bwd_s_mixed": t_mixed, "fwd_bwd_s_fp64": t_fp64,
+        "speedup": t_fp64 / t_mixed,
+        "grad_vals_rel_err_vs_fp64": (torch.linalg.norm(gv_m - gv_d) / torch.linalg.norm(gv_d)).item(),
+        "grad_b_rel_err_vs_fp64": (torch.linalg.norm(gb_m - gb_d) / torch.linalg.norm(gb_d)).item(),
+        "tolerance": 1e-10}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,7 +276,14 @@ def main():
                     help="iterations the reference arm scales to (0: measured FP64 count)")
     ap.add_argument("--ref-sample", type=int, default=128)
     ap.add_argument("--ref-sample-it", type=int, default=10)
+    ap.add_argument("--workload", default="pcg", choices=["pcg", "varcoef"],
+                    help="pcg: the headline metric; varcoef: the differentiable-solve checks")
+    ap.add_argument("--grid3", type=int, default=128)
+    ap.add_argument("--grid4", type=int, nargs=3, default=[512, 512, 256])
     args = ap.parse_args()
+    if args.workload == "varcoef":
+        run_varcoef(args)
+        return
     g = args.grid
     dims = (g[0], g[0], g[0]) if len(g) == 1 else tuple(g)
 
