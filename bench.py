@@ -307,7 +307,7 @@ def main():
     torch.cuda.set_device(dev)
 
     from hpcg_b200 import Problem
-    from hpcg_b200._lib import PROBE_GS_FINE
+    from hpcg_b200._lib import PROBE_GS_FINE, PROBE_GS_FINE_BWD, PROBE_SPMV_FINE
 
     def barrier():
         torch.cuda.synchronize()
@@ -332,11 +332,12 @@ def main():
     # ---------------- warm-up (untimed); the probe is armed first so that the
     # solver's CUDA graph (with its event nodes) is captured here, not in the
     # timed region
-    P.set_probe(PROBE_GS_FINE)
+    P.set_probe(PROBE_GS_FINE | PROBE_GS_FINE_BWD | PROBE_SPMV_FINE)
     for _ in range(args.warmup):
         solve(True)
     # ---------------- timed mixed solves
-    P.probe_read(reset=True)
+    for kind in (PROBE_GS_FINE, PROBE_GS_FINE_BWD, PROBE_SPMV_FINE):
+        P.probe_read(kind, reset=True)
     barrier()
     l0 = P.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -357,7 +358,8 @@ def main():
         wall = time.perf_counter() - t0
     launches = P.launch_count() - l0
     times = [a.elapsed_time(b_) * 1e-3 for a, b_ in ev]
-    probe_ms, probe_n, probe_bytes = P.probe_read(reset=True)
+    probes = {k: P.probe_read(k, reset=True)
+              for k in (PROBE_GS_FINE, PROBE_GS_FINE_BWD, PROBE_SPMV_FINE)}
     P.set_probe(0)
     t_mixed = statistics.mean(times)
     relres_mixed = nr / nr0
@@ -403,14 +405,23 @@ def main():
     gf_fp64 = flops * k64 / t_fp64 / 1e9
     hbm_mixed = b32 * iters_mixed[-1] / t_mixed / 1e9
     hbm_fp64 = b64 * k64 / t_fp64 / 1e9
-    achieved = probe_bytes / (probe_ms * 1e-3) / 1e9 if probe_ms > 0 else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "gs_fine_traffic.json")
-    if os.path.exists(tpath):
+    traffic = {}
+    tpath = os.path.join(ROOT, "profiles", "roofline_traffic_%d.json" % dims[0])
+    if os.path.exists(tpath) and dims[0] == dims[1] == dims[2]:
         try:
-            traffic = json.load(open(tpath)).get("bytes_per_launch_512")
+            traffic = json.load(open(tpath))
         except Exception:
-            traffic = None
+            traffic = {}
+
+    def roofline(kind, name):
+        ms, cnt, by = probes[kind]
+        ach = by / (ms * 1e-3) / 1e9 if ms > 0 else None
+        tr = traffic.get(name, {}).get("dram_bytes_per_launch") if traffic else None
+        return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": (ach / peak) if ach else None, "traffic": tr,
+                "algorithmic_bytes_per_launch": (by / cnt) if cnt else None,
+                "launches": cnt, "mean_launch_ms": (ms / cnt) if cnt else None,
+                "peak_kind": peak_kind}
 
     if rank != 0:
         if dist:
@@ -438,10 +449,9 @@ def main():
         "gflops": {"mixed": gf_mixed, "fp64": gf_fp64, "model": "src/ReportResults.cpp:81-97"},
         "hbm": {"mixed_gbs": hbm_mixed, "fp64_gbs": hbm_fp64, "mixed_frac": hbm_mixed / peak,
                 "fp64_frac": hbm_fp64 / peak, "peak_gbs": peak, "peak_kind": peak_kind},
-        "roofline": {"kernel": "k_gs_class (finest level, BF16/FP32, all modes)", "bound": "hbm",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "launches": probe_n, "peak_kind": peak_kind},
+        "roofline": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f64>"),
+        "roofline_spmv": roofline(PROBE_SPMV_FINE, "k_spmv<double,double,1>"),
+        "roofline_gs_fine_all_modes": roofline(PROBE_GS_FINE, "k_gs_class finest level, all modes"),
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8,
                 "d2h_bytes_per_step": n * 8},
         "gpu_launches": int(launches),

@@ -62,7 +62,7 @@ SIGNATURES = {
     "hpcgx_fill_uniform": (_I, [_P, _I64, _U64, _D, _D, _P]),
     "hpcgx_fill_normal": (_I, [_P, _I64, _U64, _U64, _P]),
     "hpcgx_set_probe": (_I, [_P, _I]),
-    "hpcgx_probe_read": (_I, [_P, _DP, _I64P, _DP, _I]),
+    "hpcgx_probe_read": (_I, [_P, _I, _DP, _I64P, _DP, _I]),
     "hpcgx_launch_count": (_I64, [_P]),
     "hpcgx_synchronize": (_I, [_P]),
     "hpcgx_set_stream": (_I, [_P, _P]),
@@ -71,7 +71,7 @@ SIGNATURES = {
 HPCGX_OK = 0
 ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ESTATE", 4: "ENONFINITE", 5: "ELAYOUT", 6: "ENOMEM"}
 GEN_HPCG, GEN_VARCOEF = 0, 1
-PROBE_NONE, PROBE_GS_FINE, PROBE_SPMV_FINE = 0, 1, 2
+PROBE_NONE, PROBE_GS_FINE, PROBE_SPMV_FINE, PROBE_GS_FINE_BWD = 0, 1, 2, 4
 CG_PLAIN, CG_MG, CG_MIXED = 0, 1, 2
 
 

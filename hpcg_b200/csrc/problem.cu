@@ -8,11 +8,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <memory>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -68,7 +70,10 @@ enum GraphKind { G_FP64_PREC = 0, G_FP64_NOPREC = 1, G_MIXED = 2, G_COUNT = 3 };
 struct Probe {
   cudaEvent_t a, b;
   double bytes;
+  int kind;   // one HPCGX_PROBE_* bit
 };
+
+int probe_slot(int kind) { return kind == HPCGX_PROBE_GS_FINE ? 0 : kind == HPCGX_PROBE_SPMV_FINE ? 1 : 2; }
 
 }  // namespace
 
@@ -108,8 +113,8 @@ struct hpcgx_problem {
   std::vector<Probe> probes[G_COUNT];
   std::vector<Probe> event_pool;  // created outside stream capture
   size_t pool_next = 0;
-  double probe_ms = 0.0, probe_bytes = 0.0;
-  int64_t probe_launches = 0;
+  double probe_ms[3] = {}, probe_bytes[3] = {};
+  int64_t probe_launches[3] = {};
   size_t bytes = 0;
 
   ~hpcgx_problem();
@@ -152,17 +157,23 @@ struct hpcgx_problem {
   }
 
   // ---- probed launch helpers (events only while capturing a graph)
+  // kinds: the probe bits this launch belongs to; it is bracketed by events
+  // (once) if one of them is armed and a graph is being captured.
   template <class F>
-  int probed(bool match, double bytes_model, F &&launch) {
-    const bool use = capturing && match && probe != HPCGX_PROBE_NONE;
-    if (use) {
+  int probed(int kinds, double bytes_model, F &&launch) {
+    const int armed = capturing ? (kinds & probe) : 0;
+    if (armed) {
       if (pool_next >= event_pool.size()) return fail(HPCGX_ESTATE, "probe event pool exhausted");
       Probe pr = event_pool[pool_next++];
       pr.bytes = bytes_model;
       CK(cudaEventRecordWithFlags(pr.a, stream, cudaEventRecordExternal));
       int k = launch();
       CK(cudaEventRecordWithFlags(pr.b, stream, cudaEventRecordExternal));
-      if (k) probes[capture_kind].push_back(pr);
+      for (int bit = 1; bit <= 4; bit <<= 1)
+        if (k && (armed & bit)) {
+          pr.kind = bit;
+          probes[capture_kind].push_back(pr);
+        }
       note(k);
     } else {
       note(launch());
@@ -175,8 +186,12 @@ struct hpcgx_problem {
   int gs_launch(int l, int q, int backward, int mode, const void *r, T *x, const T *xc, T *rc,
                 const int *done) {
     const bool mixed = std::is_same<T, float>::value;
-    const bool match = (probe == HPCGX_PROBE_GS_FINE && l == 0);
-    return probed(match, match ? gs_bytes(l, q, mode, mixed) : 0.0, [&]() {
+    int kinds = 0;
+    if (l == 0) {
+      kinds |= HPCGX_PROBE_GS_FINE;
+      if (mode == GS_PLAIN && backward) kinds |= HPCGX_PROBE_GS_FINE_BWD;
+    }
+    return probed(kinds, (kinds & probe) ? gs_bytes(l, q, mode, mixed) : 0.0, [&]() {
       if (l == 0)
         return launch_gs_class<T, RT0>(L[l], q, backward, mode, static_cast<const RT0 *>(r), x,
                                        xc, rc, done, stream);
@@ -276,9 +291,8 @@ struct hpcgx_problem {
       note(launch_cg_p<double>(n, z, p, st, stream));
     }
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][2], stream, cudaEventRecordExternal));
-    const bool match = probe == HPCGX_PROBE_SPMV_FINE;
     double spmv_bytes = 0.0;
-    if (match) {
+    if (probe & HPCGX_PROBE_SPMV_FINE) {
       // 12 B per real nonzero, x and y once, plus the fused p.Ap read of nothing extra
       int64_t nnz = 0;
       for (int s = 0; s < HPCGX_STENCIL; ++s) {
@@ -291,7 +305,7 @@ struct hpcgx_problem {
       }
       spmv_bytes = 12.0 * nnz + 16.0 * n;
     }
-    TRY(probed(match, spmv_bytes, [&]() {
+    TRY(probed(HPCGX_PROBE_SPMV_FINE, spmv_bytes, [&]() {
       return launch_spmv(L[0], p, Ap, &red, FIN_CG_PAP, st, done, stream);
     }));
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][3], stream, cudaEventRecordExternal));
@@ -349,9 +363,10 @@ struct hpcgx_problem {
     for (auto &pr : probes[kind]) {
       float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, pr.a, pr.b));
-      probe_ms += ms;
-      probe_bytes += pr.bytes;
-      probe_launches += 1;
+      const int slot = probe_slot(pr.kind);
+      probe_ms[slot] += ms;
+      probe_bytes[slot] += pr.bytes;
+      probe_launches[slot] += 1;
     }
     return HPCGX_OK;
   }
@@ -461,51 +476,106 @@ int check_level(hpcgx_problem *p, int level) {
   return HPCGX_OK;
 }
 
+// Runs f(begin, end) over [0, n) on the host's cores.
+template <class F>
+void parallel_for(int64_t n, F f) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(hw ? hw : 1, 64));
+  if (n < 65536 || nt == 1) {
+    f(0, n, 0);
+    return;
+  }
+  std::vector<std::thread> ts;
+  const int64_t chunk = (n + nt - 1) / nt;
+  for (int64_t t = 0; t < nt; ++t) {
+    const int64_t a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) ts.emplace_back(f, a, b, (int)t);
+  }
+  for (auto &th : ts) th.join();
+}
+
 // Shared body of the two host loaders: get(i, j, col, val) yields entry j of
-// row i.
+// row i.  Rows are validated and scattered into the device layout in
+// parallel; the first failing row (lowest index) is reported.
 template <class Nnz, class Get>
 int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
   TRY(check_level(p, level));
   LevelDev &A = p->L[level];
   const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
-  std::vector<double> vals(slots, 0.0);
-  std::vector<int32_t> cols(slots, 0);
-  for (int64_t row = 0; row < A.n; ++row) {
-    const int ix = (int)(row % A.nx), iy = (int)((row / A.nx) % A.ny),
-              iz = (int)(row / ((int64_t)A.nx * A.ny));
-    const int64_t k = storage_row_host(A, row);
-    for (int s = 0; s < HPCGX_STENCIL; ++s) cols[cidx(k, s)] = (int32_t)row;
-    const int nz = nnz_of(row);
-    if (nz < 1 || nz > HPCGX_STENCIL)
-      return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + " has " + std::to_string(nz) +
-                                     " entries");
-    int last = -1;
-    bool diag = false;
-    for (int j = 0; j < nz; ++j) {
-      int32_t col;
-      double v;
-      get(row, j, col, v);
-      if (col < 0 || col >= A.n)
-        return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + ": column out of range");
-      const int jx = col % A.nx, jy = (col / A.nx) % A.ny, jz = (int)(col / ((int64_t)A.nx * A.ny));
-      const int dx = jx - ix, dy = jy - iy, dz = jz - iz;
-      if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1)
-        return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + ": column " +
-                                       std::to_string(col) + " is not a stencil neighbour");
-      const int s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-      if (s <= last)
-        return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) +
-                                       ": entries not in stencil order");
-      last = s;
-      diag |= (s == HPCGX_DIAG_SLOT);
-      vals[vidx(k, s)] = v;
-      cols[cidx(k, s)] = col;
-    }
-    if (!diag) return fail(HPCGX_ELAYOUT, "row " + std::to_string(row) + " has no diagonal");
+  std::unique_ptr<double[]> vals(new double[slots]);
+  std::unique_ptr<int32_t[]> cols(new int32_t[slots]);
+  // rows that only pad a colour to 32 rows: value 0, column 0
+  for (int c = 0; c < 8; ++c) {
+    const int64_t end = (c < 7 ? A.cstart[c + 1] : A.storage_rows);
+    for (int64_t k = A.cstart[c] + A.ccount[c]; k < end; ++k)
+      for (int s = 0; s < HPCGX_STENCIL; ++s) {
+        vals[vidx(k, s)] = 0.0;
+        cols[cidx(k, s)] = 0;
+      }
   }
-  CK(cudaMemcpyAsync(A.vals, vals.data(), slots * sizeof(double), cudaMemcpyHostToDevice,
+  struct Err {
+    int64_t row = -1;
+    std::string msg;
+  };
+  std::vector<Err> errs(64);
+  parallel_for(A.n, [&](int64_t r0, int64_t r1, int t) {
+    for (int64_t row = r0; row < r1; ++row) {
+      const int ix = (int)(row % A.nx), iy = (int)((row / A.nx) % A.ny),
+                iz = (int)(row / ((int64_t)A.nx * A.ny));
+      const int64_t k = storage_row_host(A, row);
+      for (int s = 0; s < HPCGX_STENCIL; ++s) {
+        vals[vidx(k, s)] = 0.0;
+        cols[cidx(k, s)] = (int32_t)row;
+      }
+      auto bad = [&](const std::string &m) {
+        errs[t].row = row;
+        errs[t].msg = "row " + std::to_string(row) + ": " + m;
+      };
+      const int nz = nnz_of(row);
+      if (nz < 1 || nz > HPCGX_STENCIL) {
+        bad(std::to_string(nz) + " entries");
+        return;
+      }
+      int last = -1;
+      bool diag = false;
+      for (int j = 0; j < nz; ++j) {
+        int32_t col;
+        double v;
+        get(row, j, col, v);
+        if (col < 0 || col >= A.n) {
+          bad("column out of range");
+          return;
+        }
+        const int jx = col % A.nx, jy = (col / A.nx) % A.ny,
+                  jz = (int)(col / ((int64_t)A.nx * A.ny));
+        const int dx = jx - ix, dy = jy - iy, dz = jz - iz;
+        if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
+          bad("column " + std::to_string(col) + " is not a stencil neighbour");
+          return;
+        }
+        const int s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+        if (s <= last) {
+          bad("entries not in stencil order");
+          return;
+        }
+        last = s;
+        diag |= (s == HPCGX_DIAG_SLOT);
+        vals[vidx(k, s)] = v;
+        cols[cidx(k, s)] = col;
+      }
+      if (!diag) {
+        bad("no diagonal");
+        return;
+      }
+    }
+  });
+  const Err *first = nullptr;
+  for (const Err &e : errs)
+    if (e.row >= 0 && (!first || e.row < first->row)) first = &e;
+  if (first) return fail(HPCGX_ELAYOUT, first->msg);
+  CK(cudaMemcpyAsync(A.vals, vals.get(), slots * sizeof(double), cudaMemcpyHostToDevice,
                      p->stream));
-  CK(cudaMemcpyAsync(A.cols, cols.data(), slots * sizeof(int32_t), cudaMemcpyHostToDevice,
+  CK(cudaMemcpyAsync(A.cols, cols.get(), slots * sizeof(int32_t), cudaMemcpyHostToDevice,
                      p->stream));
   CK(cudaStreamSynchronize(p->stream));
   p->loaded[level] = true;
@@ -924,23 +994,27 @@ int hpcgx_fill_normal(hpcgx_problem *p, int64_t n, uint64_t seed, uint64_t offse
   return HPCGX_OK;
 }
 
-int hpcgx_set_probe(hpcgx_problem *p, int probe) {
+int hpcgx_set_probe(hpcgx_problem *p, int probe_mask) {
   HANDLE(p);
-  if (probe < HPCGX_PROBE_NONE || probe > HPCGX_PROBE_SPMV_FINE)
-    return fail(HPCGX_EINVAL, "unknown probe");
-  p->probe = probe;
+  if (probe_mask < 0 || probe_mask > 7) return fail(HPCGX_EINVAL, "unknown probe mask");
+  p->probe = probe_mask;
   return HPCGX_OK;
 }
 
-int hpcgx_probe_read(hpcgx_problem *p, double *ms, int64_t *launches, double *bytes, int reset) {
+int hpcgx_probe_read(hpcgx_problem *p, int kind, double *ms, int64_t *launches, double *bytes,
+                     int reset) {
   if (!p) return fail(HPCGX_EINVAL, "null problem handle");
-  if (ms) *ms = p->probe_ms;
-  if (launches) *launches = p->probe_launches;
-  if (bytes) *bytes = p->probe_bytes;
+  if (kind != HPCGX_PROBE_GS_FINE && kind != HPCGX_PROBE_SPMV_FINE &&
+      kind != HPCGX_PROBE_GS_FINE_BWD)
+    return fail(HPCGX_EINVAL, "probe_read takes a single probe kind");
+  const int slot = probe_slot(kind);
+  if (ms) *ms = p->probe_ms[slot];
+  if (launches) *launches = p->probe_launches[slot];
+  if (bytes) *bytes = p->probe_bytes[slot];
   if (reset) {
-    p->probe_ms = 0.0;
-    p->probe_bytes = 0.0;
-    p->probe_launches = 0;
+    p->probe_ms[slot] = 0.0;
+    p->probe_bytes[slot] = 0.0;
+    p->probe_launches[slot] = 0;
   }
   return HPCGX_OK;
 }

@@ -17,9 +17,11 @@ PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
 REF = os.environ.get("HPCG_REF_SRC", "/root/reference/src")
 BINARY = os.path.join(HERE, "_build", "xhpcg_b200")
-# The files HPCG expects an implementation to replace (src/*.cpp forwarding to *_ref).
+# The files HPCG expects an implementation to replace (src/*.cpp forwarding to
+# *_ref); GenerateProblem.cpp is replaced to cut set-up time (same data).
 REPLACED = ["CG.cpp", "ComputeSPMV.cpp", "ComputeSYMGS.cpp", "ComputeMG.cpp",
-            "ComputeDotProduct.cpp", "ComputeWAXPBY.cpp", "OptimizeProblem.cpp"]
+            "ComputeDotProduct.cpp", "ComputeWAXPBY.cpp", "OptimizeProblem.cpp",
+            "GenerateProblem.cpp"]
 
 
 def build(force: bool = False) -> str | None:

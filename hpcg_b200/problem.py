@@ -258,9 +258,11 @@ class Problem:
     def set_probe(self, probe):
         check(lib().hpcgx_set_probe(self.h, int(probe)))
 
-    def probe_read(self, reset=True):
+    def probe_read(self, kind=_lib.PROBE_GS_FINE, reset=True):
+        """(summed device ms, launches, algorithmic bytes) of one probe kind."""
         ms, n, b = C.c_double(), C.c_int64(), C.c_double()
-        check(lib().hpcgx_probe_read(self.h, C.byref(ms), C.byref(n), C.byref(b), int(reset)))
+        check(lib().hpcgx_probe_read(self.h, int(kind), C.byref(ms), C.byref(n), C.byref(b),
+                                     int(reset)))
         return ms.value, n.value, b.value
 
     def launch_count(self):

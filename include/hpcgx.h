@@ -196,15 +196,18 @@ int hpcgx_fill_normal(hpcgx_problem *p, int64_t n, uint64_t seed, uint64_t offse
 /* ---- measurement -------------------------------------------------------- */
 
 #define HPCGX_PROBE_NONE 0
-#define HPCGX_PROBE_GS_FINE 1   /* every finest-level Gauss-Seidel class launch */
-#define HPCGX_PROBE_SPMV_FINE 2 /* the CG SpMV (with fused p.Ap)                */
-/* Brackets the selected launches inside the solvers' CUDA graphs with CUDA
- * events; hpcgx_probe_read returns their summed device time, launch count
- * and algorithmic bytes (compulsory traffic: real nonzeros, no padding)
- * since the last reset.  Events are read at every host check of the solver,
- * so solvers run with one iteration between checks while a probe is set. */
-int hpcgx_set_probe(hpcgx_problem *p, int probe);
-int hpcgx_probe_read(hpcgx_problem *p, double *ms, int64_t *launches, double *bytes, int reset);
+#define HPCGX_PROBE_GS_FINE 1       /* every finest-level Gauss-Seidel class launch     */
+#define HPCGX_PROBE_SPMV_FINE 2     /* the CG SpMV (with fused p.Ap)                    */
+#define HPCGX_PROBE_GS_FINE_BWD 4   /* finest-level plain backward class launches only  */
+/* Brackets the selected launches (a bit mask of the kinds above) inside the
+ * solvers' CUDA graphs with CUDA events; hpcgx_probe_read returns, for one
+ * kind, their summed device time, launch count and algorithmic bytes
+ * (compulsory traffic: real nonzeros, no padding) since the last reset.
+ * Events are read at every host check of the solver, so solvers run with one
+ * iteration between checks while a probe is set. */
+int hpcgx_set_probe(hpcgx_problem *p, int probe_mask);
+int hpcgx_probe_read(hpcgx_problem *p, int kind, double *ms, int64_t *launches, double *bytes,
+                     int reset);
 /* Kernel launches issued by the library on this problem since creation. */
 int64_t hpcgx_launch_count(hpcgx_problem *p);
 /* Waits for all work of the problem's stream. */
