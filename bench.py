@@ -124,6 +124,17 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(values, dist=None, device=None):
+    """Element-wise max of a list of floats over all ranks (identity on one rank).
+    Every rank must call it with the same number of values."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return list(values)
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def cpu_reference_sample(iters_512, dims, sample_n=128, sample_it=10):
     """CG_ref of the reference build (oracle/_ref) on a sample_n^3 problem:
     per-iteration time of a bounded run, scaled to dims rows and iters_512."""
@@ -394,10 +405,7 @@ def main():
     t_e2e = time.perf_counter() - te
 
     # ---------------- max over ranks
-    if dist:
-        tt = torch.tensor([t_mixed, t_fp64, t_e2e], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_mixed, t_fp64, t_e2e = tt.tolist()
+    t_mixed, t_fp64, t_e2e = max_over_ranks([t_mixed, t_fp64, t_e2e], dist, f"cuda:{dev}")
 
     flops, b64, b32, n0, z0 = model(dims)
     peak, peak_kind = peaks()
