@@ -55,9 +55,10 @@ def peaks():
 
 
 def model(dims, levels=4):
-    """HPCG's flop model (src/ReportResults.cpp:81-97) and the compulsory-byte
-    model per iteration: SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n, R+P 40 n_c,
-    CG vectors 112 n (FP64); the mixed V-cycle moves 6 B/nnz and FP32 vectors."""
+    """HPCG's flop model (src/ReportResults.cpp:81-97) and the reference-style
+    byte model per iteration: SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n,
+    R+P 40 n_c, CG vectors 112 n (FP64); the mixed V-cycle moves 6 B/nnz (BF16
+    value + int32 column) and FP32 vectors."""
     def nnz(nx, ny, nz):
         return (3 * nx - 2) * (3 * ny - 2) * (3 * nz - 2)
     lv = [(dims[0] >> l, dims[1] >> l, dims[2] >> l) for l in range(levels)]

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 namespace hpcgx {
 
@@ -240,6 +241,29 @@ __device__ __forceinline__ void load_plane(const int32_t *__restrict__ cols, int
   if (need(9 * p + 8)) c[8] = __ldg(q + 256 + lane);
 }
 
+// Columns of one z-plane from the compressed form: base + 8-bit offset.
+template <class NEED>
+__device__ __forceinline__ void load_plane_compressed(const int32_t *__restrict__ cbase,
+                                                      const uint8_t *__restrict__ cdelta,
+                                                      int64_t k, int p, NEED need, int32_t *c) {
+  const int32_t *b = cbase + (k >> 5) * kBaseInts + p * 12;
+  const uint8_t *d = cdelta + (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (need(9 * p + 4 * j) || need(9 * p + 4 * j + 1) || need(9 * p + 4 * j + 2) ||
+        need(9 * p + 4 * j + 3)) {
+      const int4 bb = __ldg(reinterpret_cast<const int4 *>(b + 4 * j));
+      const unsigned int dd = __ldg(reinterpret_cast<const unsigned int *>(d + j * 128 + lane * 4));
+      c[4 * j] = bb.x + (int)(dd & 0xffu);
+      c[4 * j + 1] = bb.y + (int)((dd >> 8) & 0xffu);
+      c[4 * j + 2] = bb.z + (int)((dd >> 16) & 0xffu);
+      c[4 * j + 3] = bb.w + (int)(dd >> 24);
+    }
+  }
+  if (need(9 * p + 8)) c[8] = __ldg(b + 8) + (int)__ldg(d + 256 + lane);
+}
+
 struct NeedAll {
   __device__ constexpr bool operator()(int) const { return true; }
 };
@@ -305,7 +329,11 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 // PRO:  x_i first receives the prolongated coarse correction (colour 0).
 // RES:  after the update, the fine residual at this injected point is formed
 //       and restricted: rc = r_i - (A x)_i with (A x)_i summed as in SpMV.
-template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
+// SYM:  forward update of a row of the last colour, immediately followed by
+//       its backward update (the first step of the backward sweep): between
+//       the two only x_i changes, so the backward value is recomputed from the
+//       same registers and only that value is stored.
+template <bool ZERO, bool PRO, bool RES, bool SYM = false, class VT, class T, class RT>
 __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, int c,
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
                                        T *__restrict__ rc) {
@@ -313,10 +341,16 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   VT val[HPCGX_STENCIL];
   // slots whose neighbour is read: all, or (zero guess) the lower colours
   auto need = [c](int s) { return !ZERO || s == HPCGX_DIAG_SLOT || ((c ^ slot_mask(s)) < c); };
+  // the mixed V-cycle (BF16 values) reads compressed columns
+  constexpr bool COMP = std::is_same<VT, uint16_t>::value;
+  const bool wide = COMP ? __ldg(A.cwide + (id.k >> 5)) != 0 : true;
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
     load_plane(A.vals, id.k, p, need, val + 9 * p);
-    load_plane(A.cols, id.k, p, need, col + 9 * p);
+    if (COMP && !wide)
+      load_plane_compressed(A.cbase, A.cdelta, id.k, p, need, col + 9 * p);
+    else
+      load_plane(A.cols, id.k, p, need, col + 9 * p);
   }
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
@@ -346,6 +380,21 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   }
   if (!ZERO) sum = rn_add(sum, rn_mul(xi, d));
   const T xn = rn_div(sum, d);
+  if (SYM) {
+    T sum2 = rhs;
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      if (s == HPCGX_DIAG_SLOT) {
+        sum2 = rn_sub(sum2, rn_mul(d, xn));
+        continue;
+      }
+      if (col[s] == id.row) continue;   // padding slot: no term in the reference
+      sum2 = rn_sub(sum2, rn_mul(to_arith(val[s], T()), xv[s]));
+    }
+    sum2 = rn_add(sum2, rn_mul(xn, d));
+    x[id.row] = rn_div(sum2, d);
+    return;
+  }
   x[id.row] = xn;
   if (RES) {
     T ax = T(0);
@@ -386,6 +435,33 @@ k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
     }
     if (half == 0) __syncthreads();
   }
+}
+
+// The last class of a forward sweep fused with the first class of the
+// following backward sweep: colour 6 forward, colour 7 forward and backward
+// (SYM), colour 6 backward.  Class 3's colours only depend on each other
+// along x inside a line, so the block's own lines carry every dependency;
+// the matrix rows of the class are read from DRAM once instead of twice
+// (colour 6's rows come back from L2 in the last phase).
+template <bool ZERO, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads, 2)
+k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
+                const int *__restrict__ done) {
+  if (done && *done) return;
+  const int j0 = blockIdx.x * lpb;
+  const int j1 = min(j0 + lpb, C.lines);
+  const int cnt0 = (j1 - j0) * C.len[0], cnt1 = (j1 - j0) * C.len[1];
+  for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
+    gs_row<ZERO, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
+                               (T *)nullptr);
+  __syncthreads();
+  for (int t = threadIdx.x; t < cnt1; t += blockDim.x)
+    gs_row<ZERO, false, false, true>(A, row_of(C, A.nx, A.ny, 1, j0, t), 7, r, x,
+                                     (const T *)nullptr, (T *)nullptr);
+  __syncthreads();
+  for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
+    gs_row<false, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
+                                (T *)nullptr);
 }
 
 // ---------------------------------------------------------------- vectors
@@ -713,6 +789,41 @@ __global__ void k_to_bf16(int64_t m, const double *__restrict__ v, uint16_t *h) 
   }
 }
 
+// Builds the compressed columns: one warp per 32-row slice.  Rows that only
+// pad a colour to 32 take lane 0's column so that they never widen a slice.
+__global__ void k_compress_cols(Geo g, int64_t nslices, const int32_t *__restrict__ cols,
+                                int32_t *cbase, uint8_t *cdelta, uint8_t *cwide) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t sl = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); sl < nslices;
+       sl += warps) {
+    const int64_t k = sl * 32 + lane;
+    int64_t row;
+    int ix, iy, iz;
+    const bool real = storage_to_natural(g, k, row, ix, iy, iz);
+    bool ok = true;
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      int c = cols[cidx(k, s)];
+      const int c0 = __shfl_sync(0xffffffffu, c, 0);
+      if (!real) c = c0;
+      int mn = c, mx = c;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      }
+      ok = ok && (mx - mn <= 255);
+      if (lane == 0) cbase[sl * kBaseInts + (s / 9) * 12 + (s % 9)] = mn;
+      cdelta[cidx(k, s)] = (uint8_t)(mx - mn <= 255 ? c - mn : 0);
+    }
+    if (lane < 9) {   // the pad ints of each plane
+      const int p = lane / 3, i = 9 + lane % 3;
+      cbase[sl * kBaseInts + p * 12 + i] = 0;
+    }
+    if (lane == 0) cwide[sl] = ok ? 0 : 1;
+  }
+}
+
 // Values in natural row order, 27 stencil slots per row -> device layout.
 // Slots without a neighbour stay 0 whatever the input holds.
 __global__ void k_set_values(Geo g, int64_t n, const double *__restrict__ in, double *vals) {
@@ -801,6 +912,9 @@ LevelMat<VT> mat_of(const LevelDev &L, const VT *vals) {
   LevelMat<VT> A;
   A.vals = vals;
   A.cols = L.cols;
+  A.cbase = L.cbase;
+  A.cdelta = L.cdelta;
+  A.cwide = L.cwide;
   A.nx = L.nx;
   A.ny = L.ny;
   A.nz = L.nz;
@@ -902,6 +1016,15 @@ int launch_to_bf16(const LevelDev &L, cudaStream_t s) {
   return 1;
 }
 
+int launch_compress_cols(const LevelDev &L, cudaStream_t s) {
+  const int64_t nslices = L.storage_rows / 32;
+  if (nslices == 0) return 0;
+  const int64_t blocks = std::min<int64_t>((nslices + 7) / 8, 148 * 16);
+  k_compress_cols<<<(int)blocks, kThreads, 0, s>>>(geo_of(L), nslices, L.cols, L.cbase, L.cdelta,
+                                                    L.cwide);
+  return 1;
+}
+
 int launch_set_values(const LevelDev &L, const double *vals27, cudaStream_t s) {
   k_set_values<<<grid_for(L.n), kThreads, 0, s>>>(geo_of(L), L.n, vals27, L.vals);
   return 1;
@@ -963,6 +1086,14 @@ int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *
   const dim3 g(L.blocks[q]), b(L.threads[q]);
   const int lpb = L.lines_per_block[q];
   const ClassInfo &C = L.cls[q];
+  if (mode & GS_SYM3) {
+    if (q != 3) return 0;
+    if (mode & GS_ZERO_GUESS)
+      k_gs_class3_sym<true><<<g, b, 0, s>>>(A, C, lpb, r, x, done);
+    else
+      k_gs_class3_sym<false><<<g, b, 0, s>>>(A, C, lpb, r, x, done);
+    return 1;
+  }
   if (mode == GS_ZERO_GUESS && !backward) {
     switch (q) {
       case 0: k_gs_class<GS_ZERO_GUESS, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;

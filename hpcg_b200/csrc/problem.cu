@@ -133,7 +133,8 @@ struct hpcgx_problem {
   // ---- byte model of one class launch (for probes)
   double gs_bytes(int l, int q, int mode, bool mixed) const {
     const LevelDev &A = L[l];
-    const double vb = mixed ? 2.0 : 8.0, cb = 4.0, xb = mixed ? 4.0 : 8.0;
+    // mixed: BF16 value + 8-bit column offset per slot (+ the slice bases below)
+    const double vb = mixed ? 2.0 : 8.0, cb = mixed ? 1.0 : 4.0, xb = mixed ? 4.0 : 8.0;
     const double rb = (mixed && l > 0) ? 4.0 : 8.0;
     double total = 0.0;
     for (int px = 0; px < 2; ++px) {
@@ -144,11 +145,14 @@ struct hpcgx_problem {
         const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
         const int64_t cnt = axis_count(A.nx, px, dx) * axis_count(A.ny, py, dy) *
                             axis_count(A.nz, pz, dz);
-        const bool skipped = (mode & GS_ZERO_GUESS) && s != HPCGX_DIAG_SLOT &&
+        const bool skipped = (mode == GS_ZERO_GUESS) && s != HPCGX_DIAG_SLOT &&
                              ((c ^ slot_mask(s)) > c);
         nnzb += (double)cnt * (skipped ? vb : vb + cb);
       }
       double vec = rows * (rb + xb + ((mode & GS_ZERO_GUESS) ? 0.0 : xb));
+      // (GS_SYM3: the class's matrix, right-hand side and x once; the second
+      //  pass over colour 6 is served by L2)
+      if (mixed) vec += rows * 4.5;  // 144 B of slot bases per 32-row slice
       if ((mode & GS_RESTRICT) && c == 0) vec += rows * xb;
       if ((mode & GS_PROLONG) && c == 0) vec += rows * xb;
       total += nnzb + vec;
@@ -210,26 +214,33 @@ struct hpcgx_problem {
       rl[l] = l == 0 ? static_cast<const void *>(r0) : static_cast<const void *>(lvl_r(L[l], (T *)nullptr));
       xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
     }
+    // Each symmetric sweep: forward classes 0..2, class 3 forward+backward in
+    // one launch (GS_SYM3), backward classes 2..0 -- 7 launches.
     // descend: pre-smooth (zero initial guess) and restrict
     for (int l = 0; l + 1 < nlev; ++l) {
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr, done)));
-      for (int q = 3; q >= 0; --q)
+      TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr,
+                             done)));
+      for (int q = 2; q >= 0; --q)
         TRY((gs_launch<T, RT0>(l, q, 1, q == 0 ? GS_RESTRICT : GS_PLAIN, rl[l], xl[l], nullptr,
                                lvl_r(L[l + 1], (T *)nullptr), done)));
     }
     // coarsest level: one symmetric sweep from zero
     const int c = nlev - 1;
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < 3; ++q)
       TRY((gs_launch<T, RT0>(c, q, 0, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
-    for (int q = 3; q >= 0; --q)
+    TRY((gs_launch<T, RT0>(c, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr,
+                           done)));
+    for (int q = 2; q >= 0; --q)
       TRY((gs_launch<T, RT0>(c, q, 1, GS_PLAIN, rl[c], xl[c], nullptr, nullptr, done)));
     // ascend: prolongate and post-smooth
     for (int l = nlev - 2; l >= 0; --l) {
-      for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, q == 0 ? GS_PROLONG : GS_PLAIN, rl[l], xl[l],
                                lvl_x(L[l + 1], (T *)nullptr), nullptr, done)));
-      for (int q = 3; q >= 0; --q)
+      TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3, rl[l], xl[l], nullptr, nullptr, done)));
+      for (int q = 2; q >= 0; --q)
         TRY((gs_launch<T, RT0>(l, q, 1, GS_PLAIN, rl[l], xl[l], nullptr, nullptr, done)));
     }
     return HPCGX_OK;
@@ -237,8 +248,11 @@ struct hpcgx_problem {
 
   template <class T, class RT>
   int symgs(int l, const RT *r, T *x) {
-    for (int q = 0; q < 4; ++q) note(launch_gs_class<T, RT>(L[l], q, 0, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
-    for (int q = 3; q >= 0; --q) note(launch_gs_class<T, RT>(L[l], q, 1, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
+    for (int q = 0; q < 3; ++q)
+      note(launch_gs_class<T, RT>(L[l], q, 0, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
+    note(launch_gs_class<T, RT>(L[l], 3, 0, GS_SYM3, r, x, nullptr, nullptr, nullptr, stream));
+    for (int q = 2; q >= 0; --q)
+      note(launch_gs_class<T, RT>(L[l], q, 1, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
     return HPCGX_OK;
   }
 
@@ -262,8 +276,16 @@ struct hpcgx_problem {
       if (!loaded[l]) return fail(HPCGX_ESTATE, "matrix level " + std::to_string(l) + " not loaded");
     if (mixed && (!mixed_ready || mixed_stale)) {
       for (int l = 0; l < nlev; ++l) {
-        if (!L[l].vals16) TRY(alloc((void **)&L[l].vals16, L[l].storage_rows * HPCGX_STENCIL * 2));
-        note(launch_to_bf16(L[l], stream));
+        LevelDev &A = L[l];
+        const int64_t nslices = A.storage_rows / 32;
+        if (!A.vals16) TRY(alloc((void **)&A.vals16, A.storage_rows * HPCGX_STENCIL * 2));
+        if (!A.cdelta) {
+          TRY(alloc((void **)&A.cdelta, A.storage_rows * HPCGX_STENCIL));
+          TRY(alloc((void **)&A.cbase, std::max<int64_t>(nslices, 1) * kBaseInts * 4));
+          TRY(alloc((void **)&A.cwide, std::max<int64_t>(nslices, 1)));
+        }
+        note(launch_to_bf16(A, stream));
+        note(launch_compress_cols(A, stream));
       }
       mixed_ready = true;
       mixed_stale = false;
@@ -448,6 +470,9 @@ hpcgx_problem::~hpcgx_problem() {
     cudaFree(L[l].vals);
     cudaFree(L[l].cols);
     cudaFree(L[l].vals16);
+    cudaFree(L[l].cbase);
+    cudaFree(L[l].cdelta);
+    cudaFree(L[l].cwide);
     cudaFree(L[l].r64);
     cudaFree(L[l].x64);
     cudaFree(L[l].r32);
