@@ -52,17 +52,14 @@ struct LevelMat {
   const int32_t *cols;
   int nx, ny, nz;
   int64_t n;
-  // Compressed columns of the mixed-precision V-cycle (null elsewhere): per
-  // 32-row slice and slot an int32 base (the smallest column of the 32 rows)
-  // and one 8-bit offset per row; slices whose columns span more than 255
-  // are flagged wide and read `cols` instead.
-  const int32_t *cbase;   // [slice][3 planes][12]: slots 9p..9p+8, 3 pad
-  const uint8_t *cdelta;  // offsets, same slot grouping as cidx()
-  const uint8_t *cwide;   // [slice]: 1 = use cols
+  // Stencil offsets: slot s of row i holds column i + off[s] whenever the row
+  // has that neighbour (the layout enforces it when a level is loaded).  The
+  // mixed-precision V-cycle derives its columns from these instead of
+  // reading `cols` (slots without a neighbour hold value 0; their derived
+  // column is clamped into the matrix so that the multiplication by 0 reads
+  // valid memory).
+  int off[HPCGX_STENCIL];
 };
-
-// Ints per slice of the compressed-column bases (3 planes x 12).
-constexpr int kBaseInts = 36;
 
 // Elements of one 32-row slice and of one z-plane inside it.
 constexpr int kSliceElems = HPCGX_STENCIL * HPCGX_SLICE;  // 864

@@ -22,6 +22,7 @@
 #include "kernels.cuh"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <type_traits>
 
@@ -241,29 +242,6 @@ __device__ __forceinline__ void load_plane(const int32_t *__restrict__ cols, int
   if (need(9 * p + 8)) c[8] = __ldg(q + 256 + lane);
 }
 
-// Columns of one z-plane from the compressed form: base + 8-bit offset.
-template <class NEED>
-__device__ __forceinline__ void load_plane_compressed(const int32_t *__restrict__ cbase,
-                                                      const uint8_t *__restrict__ cdelta,
-                                                      int64_t k, int p, NEED need, int32_t *c) {
-  const int32_t *b = cbase + (k >> 5) * kBaseInts + p * 12;
-  const uint8_t *d = cdelta + (k >> 5) * kSliceElems + p * kPlaneElems;
-  const int lane = (int)(k & 31);
-#pragma unroll
-  for (int j = 0; j < 2; ++j) {
-    if (need(9 * p + 4 * j) || need(9 * p + 4 * j + 1) || need(9 * p + 4 * j + 2) ||
-        need(9 * p + 4 * j + 3)) {
-      const int4 bb = __ldg(reinterpret_cast<const int4 *>(b + 4 * j));
-      const unsigned int dd = __ldg(reinterpret_cast<const unsigned int *>(d + j * 128 + lane * 4));
-      c[4 * j] = bb.x + (int)(dd & 0xffu);
-      c[4 * j + 1] = bb.y + (int)((dd >> 8) & 0xffu);
-      c[4 * j + 2] = bb.z + (int)((dd >> 16) & 0xffu);
-      c[4 * j + 3] = bb.w + (int)(dd >> 24);
-    }
-  }
-  if (need(9 * p + 8)) c[8] = __ldg(b + 8) + (int)__ldg(d + 256 + lane);
-}
-
 struct NeedAll {
   __device__ constexpr bool operator()(int) const { return true; }
 };
@@ -341,16 +319,20 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   VT val[HPCGX_STENCIL];
   // slots whose neighbour is read: all, or (zero guess) the lower colours
   auto need = [c](int s) { return !ZERO || s == HPCGX_DIAG_SLOT || ((c ^ slot_mask(s)) < c); };
-  // the mixed V-cycle (BF16 values) reads compressed columns
-  constexpr bool COMP = std::is_same<VT, uint16_t>::value;
-  const bool wide = COMP ? __ldg(A.cwide + (id.k >> 5)) != 0 : true;
+  // The mixed V-cycle (BF16 values) derives its columns from the stencil
+  // offsets; the FP64 path reads the stored int32 columns.
+  constexpr bool IMPLICIT = std::is_same<VT, uint16_t>::value;
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
     load_plane(A.vals, id.k, p, need, val + 9 * p);
-    if (COMP && !wide)
-      load_plane_compressed(A.cbase, A.cdelta, id.k, p, need, col + 9 * p);
-    else
-      load_plane(A.cols, id.k, p, need, col + 9 * p);
+    if (!IMPLICIT) load_plane(A.cols, id.k, p, need, col + 9 * p);
+  }
+  if (IMPLICIT) {
+    const int64_t last = A.n - 1;
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s)
+      if (need(s))
+        col[s] = (int32_t)min(max(id.row + (int64_t)A.off[s], (int64_t)0), last);
   }
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
@@ -360,12 +342,15 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   }
   T xi = ZERO ? T(0) : x[id.row];
   if (PRO) xi = rn_add(xi, __ldg(xc + crow));
+  // A slot without a neighbour holds value 0 (its column is the row itself,
+  // or, in the mixed V-cycle, a clamped derived column); in the zero-guess sweep
+  // x may be unwritten there, so its term -- a product with 0 -- is skipped.
   T xv[HPCGX_STENCIL];
 #pragma unroll
   for (int s = 0; s < HPCGX_STENCIL; ++s) {
     if (s == HPCGX_DIAG_SLOT) continue;
     if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
-    xv[s] = (ZERO && col[s] == id.row) ? T(0) : x[col[s]];
+    xv[s] = (ZERO && to_arith(val[s], T()) == T(0)) ? T(0) : x[col[s]];
   }
   T sum = rhs;
   const T d = to_arith(val[HPCGX_DIAG_SLOT], T());
@@ -375,7 +360,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
       if (!ZERO) sum = rn_sub(sum, rn_mul(d, xi));
       continue;
     }
-    if (ZERO && (((c ^ slot_mask(s)) > c) || col[s] == id.row)) continue;
+    if (ZERO && (((c ^ slot_mask(s)) > c) || to_arith(val[s], T()) == T(0))) continue;
     sum = rn_sub(sum, rn_mul(to_arith(val[s], T()), xv[s]));
   }
   if (!ZERO) sum = rn_add(sum, rn_mul(xi, d));
@@ -388,7 +373,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
         sum2 = rn_sub(sum2, rn_mul(d, xn));
         continue;
       }
-      if (col[s] == id.row) continue;   // padding slot: no term in the reference
+      if (to_arith(val[s], T()) == T(0)) continue;   // a product with 0: no change
       sum2 = rn_sub(sum2, rn_mul(to_arith(val[s], T()), xv[s]));
     }
     sum2 = rn_add(sum2, rn_mul(xn, d));
@@ -410,8 +395,14 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
 // launch; GS_PROLONG and GS_RESTRICT act on colour 0 only.  QS >= 0 fixes the
 // class at compile time, which lets the zero-guess sweep drop the loads of the
 // skipped slots statically.
+// Occupancy: the FP64 sweeps stream 12 B per slot and saturate HBM with two
+// 256-thread blocks per SM; the BF16 sweeps read 2 B per slot and are latency
+// bound, so they are held to 85 registers for three blocks per SM.
+template <class VT>
+constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 3 : 2; }
+
 template <int MODE, int DIR, int QS, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
 k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
            const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
   if (done && *done) return;
@@ -444,7 +435,7 @@ k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
 // the matrix rows of the class are read from DRAM once instead of twice
 // (colour 6's rows come back from L2 in the last phase).
 template <bool ZERO, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
 k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
                 const int *__restrict__ done) {
   if (done && *done) return;
@@ -789,41 +780,6 @@ __global__ void k_to_bf16(int64_t m, const double *__restrict__ v, uint16_t *h) 
   }
 }
 
-// Builds the compressed columns: one warp per 32-row slice.  Rows that only
-// pad a colour to 32 take lane 0's column so that they never widen a slice.
-__global__ void k_compress_cols(Geo g, int64_t nslices, const int32_t *__restrict__ cols,
-                                int32_t *cbase, uint8_t *cdelta, uint8_t *cwide) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t sl = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); sl < nslices;
-       sl += warps) {
-    const int64_t k = sl * 32 + lane;
-    int64_t row;
-    int ix, iy, iz;
-    const bool real = storage_to_natural(g, k, row, ix, iy, iz);
-    bool ok = true;
-    for (int s = 0; s < HPCGX_STENCIL; ++s) {
-      int c = cols[cidx(k, s)];
-      const int c0 = __shfl_sync(0xffffffffu, c, 0);
-      if (!real) c = c0;
-      int mn = c, mx = c;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-        mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-      }
-      ok = ok && (mx - mn <= 255);
-      if (lane == 0) cbase[sl * kBaseInts + (s / 9) * 12 + (s % 9)] = mn;
-      cdelta[cidx(k, s)] = (uint8_t)(mx - mn <= 255 ? c - mn : 0);
-    }
-    if (lane < 9) {   // the pad ints of each plane
-      const int p = lane / 3, i = 9 + lane % 3;
-      cbase[sl * kBaseInts + p * 12 + i] = 0;
-    }
-    if (lane == 0) cwide[sl] = ok ? 0 : 1;
-  }
-}
-
 // Values in natural row order, 27 stencil slots per row -> device layout.
 // Slots without a neighbour stay 0 whatever the input holds.
 __global__ void k_set_values(Geo g, int64_t n, const double *__restrict__ in, double *vals) {
@@ -912,9 +868,8 @@ LevelMat<VT> mat_of(const LevelDev &L, const VT *vals) {
   LevelMat<VT> A;
   A.vals = vals;
   A.cols = L.cols;
-  A.cbase = L.cbase;
-  A.cdelta = L.cdelta;
-  A.cwide = L.cwide;
+  for (int s = 0; s < HPCGX_STENCIL; ++s)
+    A.off[s] = (s / 9 - 1) * L.nx * L.ny + ((s / 3) % 3 - 1) * L.nx + (s % 3 - 1);
   A.nx = L.nx;
   A.ny = L.ny;
   A.nz = L.nz;
@@ -1013,15 +968,6 @@ int launch_coarsen_varcoef(const LevelDev &F, const LevelDev &Cc, cudaStream_t s
 int launch_to_bf16(const LevelDev &L, cudaStream_t s) {
   const int64_t m = L.storage_rows * HPCGX_STENCIL;
   k_to_bf16<<<grid_for(m), kThreads, 0, s>>>(m, L.vals, L.vals16);
-  return 1;
-}
-
-int launch_compress_cols(const LevelDev &L, cudaStream_t s) {
-  const int64_t nslices = L.storage_rows / 32;
-  if (nslices == 0) return 0;
-  const int64_t blocks = std::min<int64_t>((nslices + 7) / 8, 148 * 16);
-  k_compress_cols<<<(int)blocks, kThreads, 0, s>>>(geo_of(L), nslices, L.cols, L.cbase, L.cdelta,
-                                                    L.cwide);
   return 1;
 }
 

@@ -16,9 +16,6 @@ struct LevelDev {
   double *vals = nullptr;     // storage_rows*27, FP64
   int32_t *cols = nullptr;    // storage_rows*27
   uint16_t *vals16 = nullptr; // storage_rows*27, BF16 (mixed precision)
-  int32_t *cbase = nullptr;   // compressed columns of the mixed V-cycle (see LevelMat)
-  uint8_t *cdelta = nullptr;
-  uint8_t *cwide = nullptr;
   // multigrid work vectors of this level (levels >= 1: right-hand side and
   // correction; level 0 uses the caller's vectors)
   double *r64 = nullptr, *x64 = nullptr;
@@ -73,7 +70,6 @@ int launch_generate_varcoef(const LevelDev &L, int level, int nx0, int ny0, uint
                              double sigma, cudaStream_t s);
 int launch_coarsen_varcoef(const LevelDev &F, const LevelDev &Cc, cudaStream_t s);
 int launch_to_bf16(const LevelDev &L, cudaStream_t s);
-int launch_compress_cols(const LevelDev &L, cudaStream_t s);
 int launch_set_values(const LevelDev &L, const double *vals27, cudaStream_t s);
 int launch_get_values(const LevelDev &L, double *vals27, int32_t *cols27, cudaStream_t s);
 int launch_set_diagonal(const LevelDev &L, const double *diag, cudaStream_t s);

@@ -133,8 +133,8 @@ struct hpcgx_problem {
   // ---- byte model of one class launch (for probes)
   double gs_bytes(int l, int q, int mode, bool mixed) const {
     const LevelDev &A = L[l];
-    // mixed: BF16 value + 8-bit column offset per slot (+ the slice bases below)
-    const double vb = mixed ? 2.0 : 8.0, cb = mixed ? 1.0 : 4.0, xb = mixed ? 4.0 : 8.0;
+    // mixed: BF16 value per slot, columns derived from the stencil offsets
+    const double vb = mixed ? 2.0 : 8.0, cb = mixed ? 0.0 : 4.0, xb = mixed ? 4.0 : 8.0;
     const double rb = (mixed && l > 0) ? 4.0 : 8.0;
     double total = 0.0;
     for (int px = 0; px < 2; ++px) {
@@ -152,7 +152,6 @@ struct hpcgx_problem {
       double vec = rows * (rb + xb + ((mode & GS_ZERO_GUESS) ? 0.0 : xb));
       // (GS_SYM3: the class's matrix, right-hand side and x once; the second
       //  pass over colour 6 is served by L2)
-      if (mixed) vec += rows * 4.5;  // 144 B of slot bases per 32-row slice
       if ((mode & GS_RESTRICT) && c == 0) vec += rows * xb;
       if ((mode & GS_PROLONG) && c == 0) vec += rows * xb;
       total += nnzb + vec;
@@ -277,15 +276,8 @@ struct hpcgx_problem {
     if (mixed && (!mixed_ready || mixed_stale)) {
       for (int l = 0; l < nlev; ++l) {
         LevelDev &A = L[l];
-        const int64_t nslices = A.storage_rows / 32;
         if (!A.vals16) TRY(alloc((void **)&A.vals16, A.storage_rows * HPCGX_STENCIL * 2));
-        if (!A.cdelta) {
-          TRY(alloc((void **)&A.cdelta, A.storage_rows * HPCGX_STENCIL));
-          TRY(alloc((void **)&A.cbase, std::max<int64_t>(nslices, 1) * kBaseInts * 4));
-          TRY(alloc((void **)&A.cwide, std::max<int64_t>(nslices, 1)));
-        }
         note(launch_to_bf16(A, stream));
-        note(launch_compress_cols(A, stream));
       }
       mixed_ready = true;
       mixed_stale = false;
@@ -470,9 +462,6 @@ hpcgx_problem::~hpcgx_problem() {
     cudaFree(L[l].vals);
     cudaFree(L[l].cols);
     cudaFree(L[l].vals16);
-    cudaFree(L[l].cbase);
-    cudaFree(L[l].cdelta);
-    cudaFree(L[l].cwide);
     cudaFree(L[l].r64);
     cudaFree(L[l].x64);
     cudaFree(L[l].r32);
