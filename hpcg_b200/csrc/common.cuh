@@ -35,6 +35,29 @@ namespace hpcgx {
 // Largest number of multigrid levels (the reference fixes 4, src/main.cpp:139).
 constexpr int kMaxLevels = 4;
 
+// Division of n in [0, 2^31) by a fixed d >= 1 with one multiply-high, one
+// add and one shift (the round-up method of Granlund and Montgomery,
+// "Division by invariant integers using multiplication", 1994): the kernels
+// map a thread to its line and row without integer division instructions.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{d, 0u, 0u};
+  if (d == 0) return f;
+  while ((1ull << f.s) < d) ++f.s;
+  f.m = (uint32_t)(((1ull << 32) * ((1ull << f.s) - d)) / d + 1);
+  return f;
+}
+__host__ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f) {
+#ifdef __CUDA_ARCH__
+  const uint32_t hi = __umulhi(n, f.m);
+#else
+  const uint32_t hi = (uint32_t)(((uint64_t)n * f.m) >> 32);
+#endif
+  return (uint32_t)(((uint64_t)hi + n) >> f.s);
+}
+
 // The four x-line classes of a level: class q = (iy&1) + 2(iz&1).  Class q
 // holds colours 2q (even ix) and 2q+1 (odd ix).
 struct ClassInfo {
@@ -43,6 +66,8 @@ struct ClassInfo {
   int lines;        // lines of this class
   int len[2];       // rows per line for px = 0 / 1
   int64_t start[2]; // storage row of the first row of colour 2q+px
+  FastDiv dlen[2];  // division by len[px]
+  FastDiv dnyq;     // division by nyq
 };
 
 // What a kernel needs to know about one level's matrix.

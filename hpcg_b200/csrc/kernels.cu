@@ -171,12 +171,13 @@ struct RowId {
 __device__ __forceinline__ RowId row_of(const ClassInfo &C, int nx, int ny, int px, int j0,
                                         int t) {
   const int Lp = C.len[px];
-  const int jl = t / Lp;
+  const int jl = (int)fdiv((uint32_t)t, C.dlen[px]);
   const int pos = t - jl * Lp;
   const int j = j0 + jl;
+  const int jz = (int)fdiv((uint32_t)j, C.dnyq);
   RowId r;
-  r.iy = C.py + 2 * (j % C.nyq);
-  r.iz = C.pz + 2 * (j / C.nyq);
+  r.iy = C.py + 2 * (j - jz * C.nyq);
+  r.iz = C.pz + 2 * jz;
   r.ix = px + 2 * pos;
   r.row = ((int64_t)r.iz * ny + r.iy) * nx + r.ix;
   r.k = C.start[px] + (int64_t)j * Lp + pos;
@@ -240,6 +241,37 @@ __device__ __forceinline__ void load_plane(const int32_t *__restrict__ cols, int
     }
   }
   if (need(9 * p + 8)) c[8] = __ldg(q + 256 + lane);
+}
+
+// BF16 values of one z-plane straight to FP32 (a BF16 pattern is the high
+// half of the FP32 pattern of the same number).
+template <class NEED>
+__device__ __forceinline__ void load_plane_f32(const uint16_t *__restrict__ vals, int64_t k, int p,
+                                               NEED need, float *v) {
+  const uint16_t *q = vals + (k >> 5) * kSliceElems + p * kPlaneElems;
+  const int lane = (int)(k & 31);
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    if (need(9 * p + 4 * j) || need(9 * p + 4 * j + 1) || need(9 * p + 4 * j + 2) ||
+        need(9 * p + 4 * j + 3)) {
+      const uint2 t = __ldg(reinterpret_cast<const uint2 *>(q + j * 128 + lane * 4));
+      v[4 * j] = __uint_as_float(t.x << 16);
+      v[4 * j + 1] = __uint_as_float(t.x & 0xffff0000u);
+      v[4 * j + 2] = __uint_as_float(t.y << 16);
+      v[4 * j + 3] = __uint_as_float(t.y & 0xffff0000u);
+    }
+  }
+  if (need(9 * p + 8)) v[8] = __uint_as_float((uint32_t)__ldg(q + 256 + lane) << 16);
+}
+template <class NEED>
+__device__ __forceinline__ void load_vals(const double *__restrict__ vals, int64_t k, int p,
+                                          NEED need, double *v) {
+  load_plane(vals, k, p, need, v);
+}
+template <class NEED>
+__device__ __forceinline__ void load_vals(const uint16_t *__restrict__ vals, int64_t k, int p,
+                                          NEED need, float *v) {
+  load_plane_f32(vals, k, p, need, v);
 }
 
 struct NeedAll {
@@ -316,7 +348,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
                                        T *__restrict__ rc) {
   int32_t col[HPCGX_STENCIL];
-  VT val[HPCGX_STENCIL];
+  T val[HPCGX_STENCIL];   // values converted to the arithmetic type as loaded
   // slots whose neighbour is read: all, or (zero guess) the lower colours
   auto need = [c](int s) { return !ZERO || s == HPCGX_DIAG_SLOT || ((c ^ slot_mask(s)) < c); };
   // The mixed V-cycle (BF16 values) derives its columns from the stencil
@@ -324,15 +356,29 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   constexpr bool IMPLICIT = std::is_same<VT, uint16_t>::value;
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
-    load_plane(A.vals, id.k, p, need, val + 9 * p);
+    load_vals(A.vals, id.k, p, need, val + 9 * p);
     if (!IMPLICIT) load_plane(A.cols, id.k, p, need, col + 9 * p);
   }
   if (IMPLICIT) {
-    const int64_t last = A.n - 1;
+    // 32-bit row + offset; only rows on the grid boundary can point outside
+    // the vector, and only from slots whose value is 0: those read the row
+    // itself instead.
+    const int r32 = (int)id.row;
+    const bool inner = id.ix > 0 && id.ix + 1 < A.nx && id.iy > 0 && id.iy + 1 < A.ny &&
+                       id.iz > 0 && id.iz + 1 < A.nz;
+    if (inner) {
 #pragma unroll
-    for (int s = 0; s < HPCGX_STENCIL; ++s)
-      if (need(s))
-        col[s] = (int32_t)min(max(id.row + (int64_t)A.off[s], (int64_t)0), last);
+      for (int s = 0; s < HPCGX_STENCIL; ++s)
+        if (need(s)) col[s] = r32 + A.off[s];
+    } else {
+      const uint32_t n32 = (uint32_t)A.n;
+#pragma unroll
+      for (int s = 0; s < HPCGX_STENCIL; ++s)
+        if (need(s)) {
+          const int cc = r32 + A.off[s];
+          col[s] = (uint32_t)cc < n32 ? cc : r32;
+        }
+    }
   }
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
@@ -350,18 +396,18 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   for (int s = 0; s < HPCGX_STENCIL; ++s) {
     if (s == HPCGX_DIAG_SLOT) continue;
     if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
-    xv[s] = (ZERO && to_arith(val[s], T()) == T(0)) ? T(0) : x[col[s]];
+    xv[s] = (ZERO && val[s] == T(0)) ? T(0) : x[col[s]];
   }
   T sum = rhs;
-  const T d = to_arith(val[HPCGX_DIAG_SLOT], T());
+  const T d = val[HPCGX_DIAG_SLOT];
 #pragma unroll
   for (int s = 0; s < HPCGX_STENCIL; ++s) {
     if (s == HPCGX_DIAG_SLOT) {
       if (!ZERO) sum = rn_sub(sum, rn_mul(d, xi));
       continue;
     }
-    if (ZERO && (((c ^ slot_mask(s)) > c) || to_arith(val[s], T()) == T(0))) continue;
-    sum = rn_sub(sum, rn_mul(to_arith(val[s], T()), xv[s]));
+    if (ZERO && (((c ^ slot_mask(s)) > c) || val[s] == T(0))) continue;
+    sum = rn_sub(sum, rn_mul(val[s], xv[s]));
   }
   if (!ZERO) sum = rn_add(sum, rn_mul(xi, d));
   const T xn = rn_div(sum, d);
@@ -373,8 +419,8 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
         sum2 = rn_sub(sum2, rn_mul(d, xn));
         continue;
       }
-      if (to_arith(val[s], T()) == T(0)) continue;   // a product with 0: no change
-      sum2 = rn_sub(sum2, rn_mul(to_arith(val[s], T()), xv[s]));
+      if (val[s] == T(0)) continue;   // a product with 0: no change
+      sum2 = rn_sub(sum2, rn_mul(val[s], xv[s]));
     }
     sum2 = rn_add(sum2, rn_mul(xn, d));
     x[id.row] = rn_div(sum2, d);
@@ -385,7 +431,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
     T ax = T(0);
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s)
-      ax = rn_add(ax, rn_mul(to_arith(val[s], T()), s == HPCGX_DIAG_SLOT ? xn : xv[s]));
+      ax = rn_add(ax, rn_mul(val[s], s == HPCGX_DIAG_SLOT ? xn : xv[s]));
     rc[crow] = rn_sub(rhs, ax);
   }
 }
@@ -927,6 +973,9 @@ void plan_level(LevelDev &L, int nx, int ny, int nz) {
     C.len[1] = nx / 2;
     C.start[0] = L.cstart[2 * q];
     C.start[1] = L.cstart[2 * q + 1];
+    C.dlen[0] = make_fastdiv((uint32_t)C.len[0]);
+    C.dlen[1] = make_fastdiv((uint32_t)C.len[1]);
+    C.dnyq = make_fastdiv((uint32_t)C.nyq);
     const int len = std::max(C.len[0], 1);
     int lpb = std::max(1, kThreads / len);
     lpb = std::min(lpb, std::max(C.lines, 1));
