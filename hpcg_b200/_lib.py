@@ -39,6 +39,7 @@ SIGNATURES = {
     "hpcgx_memory_bytes": (_I, [_P, _DP]),
     "hpcgx_rows": (_I64, [_P, _I]),
     "hpcgx_spmv": (_I, [_P, _I, _P, _P]),
+    "hpcgx_spmv_stencil": (_I, [_P, _I, _P, _P]),
     "hpcgx_symgs": (_I, [_P, _I, _P, _P]),
     "hpcgx_mg": (_I, [_P, _P, _P]),
     "hpcgx_restriction": (_I, [_P, _I, _P, _P, _P]),

@@ -280,11 +280,46 @@ struct NeedAll {
 
 // ---------------------------------------------------------------- SpMV
 
+// Columns of storage row id derived from the stencil offsets, row + off[s] in
+// 32-bit arithmetic (vectors hold fewer than 2^31 rows).  Every level matrix
+// is a 27-point stencil matrix (the loaders reject any other pattern) whose
+// absent neighbours hold the value 0, so the stored int32 columns carry no
+// information: an interior row reads exactly row + off[s]; a row on the grid
+// boundary reads row + off[s] where that lies inside the vector and the row
+// itself elsewhere, and every slot that is not a neighbour multiplies by 0.
+template <class VT, class NEED>
+__device__ __forceinline__ void stencil_cols(const LevelMat<VT> &A, const RowId &id, NEED need,
+                                             int32_t *col) {
+  const int r32 = (int)id.row;
+  const bool inner = id.ix > 0 && id.ix + 1 < A.nx && id.iy > 0 && id.iy + 1 < A.ny &&
+                     id.iz > 0 && id.iz + 1 < A.nz;
+  if (inner) {
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s)
+      if (need(s)) col[s] = r32 + A.off[s];
+  } else {
+    const uint32_t n32 = (uint32_t)A.n;
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s)
+      if (need(s)) {
+        const int cc = r32 + A.off[s];
+        col[s] = (uint32_t)cc < n32 ? cc : r32;
+      }
+  }
+}
+
 // y = A x, rows summed left to right over the slots as ComputeSPMV_ref does
 // (src/ComputeSPMV_ref.cpp:64-70).  With DOT, also reduces sum_i x_i y_i (the
-// p.Ap of CG, src/CG.cpp:119) and runs the finishing scalar step.
-template <class VT, class T, bool DOT>
-__global__ void __launch_bounds__(kThreads, 2)
+// p.Ap of CG, src/CG.cpp:119) and runs the finishing scalar step.  IMPL
+// derives the columns from the stencil offsets instead of reading them.
+// Occupancy: with stored columns a row keeps 54 loads in flight and two
+// blocks per SM saturate HBM; without column loads the gathers issue at once
+// and four blocks per SM (64 registers) hide their latency better.
+template <bool IMPL>
+constexpr int spmv_min_blocks() { return IMPL ? 4 : 2; }
+
+template <class VT, class T, bool DOT, bool IMPL>
+__global__ void __launch_bounds__(kThreads, spmv_min_blocks<IMPL>())
 k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, Reduce red,
        int fin, void *fin_target, const int *__restrict__ done) {
   if (done && *done) return;
@@ -304,9 +339,10 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
       VT val[HPCGX_STENCIL];
 #pragma unroll
       for (int p = 0; p < 3; ++p) {
-        load_plane(A.cols, id.k, p, NeedAll(), col + 9 * p);
+        if (!IMPL) load_plane(A.cols, id.k, p, NeedAll(), col + 9 * p);
         load_plane(A.vals, id.k, p, NeedAll(), val + 9 * p);
       }
+      if (IMPL) stencil_cols(A, id, NeedAll(), col);
       T xv[HPCGX_STENCIL];
 #pragma unroll
       for (int s = 0; s < HPCGX_STENCIL; ++s) xv[s] = __ldg(x + col[s]);
@@ -359,27 +395,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
     load_vals(A.vals, id.k, p, need, val + 9 * p);
     if (!IMPLICIT) load_plane(A.cols, id.k, p, need, col + 9 * p);
   }
-  if (IMPLICIT) {
-    // 32-bit row + offset; only rows on the grid boundary can point outside
-    // the vector, and only from slots whose value is 0: those read the row
-    // itself instead.
-    const int r32 = (int)id.row;
-    const bool inner = id.ix > 0 && id.ix + 1 < A.nx && id.iy > 0 && id.iy + 1 < A.ny &&
-                       id.iz > 0 && id.iz + 1 < A.nz;
-    if (inner) {
-#pragma unroll
-      for (int s = 0; s < HPCGX_STENCIL; ++s)
-        if (need(s)) col[s] = r32 + A.off[s];
-    } else {
-      const uint32_t n32 = (uint32_t)A.n;
-#pragma unroll
-      for (int s = 0; s < HPCGX_STENCIL; ++s)
-        if (need(s)) {
-          const int cc = r32 + A.off[s];
-          col[s] = (uint32_t)cc < n32 ? cc : r32;
-        }
-    }
-  }
+  if (IMPLICIT) stencil_cols(A, id, need, col);
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
   if (PRO || RES) {
@@ -443,9 +459,10 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
 // skipped slots statically.
 // Occupancy: the FP64 sweeps stream 12 B per slot and saturate HBM with two
 // 256-thread blocks per SM; the BF16 sweeps read 2 B per slot and are latency
-// bound, so they are held to 85 registers for three blocks per SM.
+// bound, so they are held to 64 registers for four blocks per SM (five,
+// at 48 registers, spill and run slower).
 template <class VT>
-constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 3 : 2; }
+constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 4 : 2; }
 
 template <int MODE, int DIR, int QS, class VT, class T, class RT>
 __global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
@@ -1041,20 +1058,28 @@ int launch_get_diagonal(const LevelDev &L, double *diag, cudaStream_t s) {
 }
 
 int launch_spmv(const LevelDev &L, const double *x, double *y, const Reduce *dot, int fin,
-                void *fin_target, const int *done, cudaStream_t s) {
+                void *fin_target, const int *done, cudaStream_t s, bool implicit_cols) {
   if (L.spmv_blocks == 0) return 0;
-  if (dot)
-    k_spmv<double, double, true><<<L.spmv_blocks, kThreads, 0, s>>>(
-        mat_of(L, L.vals), classes_of(L), x, y, *dot, fin, fin_target, done);
+  const LevelMat<double> A = mat_of(L, L.vals);
+  const Reduce red = dot ? *dot : Reduce();
+  if (dot && implicit_cols)
+    k_spmv<double, double, true, true><<<L.spmv_blocks, kThreads, 0, s>>>(
+        A, classes_of(L), x, y, red, fin, fin_target, done);
+  else if (dot)
+    k_spmv<double, double, true, false><<<L.spmv_blocks, kThreads, 0, s>>>(
+        A, classes_of(L), x, y, red, fin, fin_target, done);
+  else if (implicit_cols)
+    k_spmv<double, double, false, true><<<L.spmv_blocks, kThreads, 0, s>>>(
+        A, classes_of(L), x, y, red, 0, nullptr, done);
   else
-    k_spmv<double, double, false><<<L.spmv_blocks, kThreads, 0, s>>>(
-        mat_of(L, L.vals), classes_of(L), x, y, Reduce(), 0, nullptr, done);
+    k_spmv<double, double, false, false><<<L.spmv_blocks, kThreads, 0, s>>>(
+        A, classes_of(L), x, y, red, 0, nullptr, done);
   return 1;
 }
 
 int launch_spmv32(const LevelDev &L, const float *x, float *y, cudaStream_t s) {
   if (L.spmv_blocks == 0) return 0;
-  k_spmv<uint16_t, float, false><<<L.spmv_blocks, kThreads, 0, s>>>(
+  k_spmv<uint16_t, float, false, true><<<L.spmv_blocks, kThreads, 0, s>>>(
       mat_of(L, L.vals16), classes_of(L), x, y, Reduce(), 0, nullptr, nullptr);
   return 1;
 }

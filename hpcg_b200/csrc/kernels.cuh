@@ -76,8 +76,9 @@ int launch_set_diagonal(const LevelDev &L, const double *diag, cudaStream_t s);
 int launch_get_diagonal(const LevelDev &L, double *diag, cudaStream_t s);
 
 // Operators ---------------------------------------------------------------
+// implicit_cols: columns from the stencil offsets (no int32 column reads).
 int launch_spmv(const LevelDev &L, const double *x, double *y, const Reduce *dot, int fin,
-                 void *fin_target, const int *done, cudaStream_t s);
+                 void *fin_target, const int *done, cudaStream_t s, bool implicit_cols = false);
 int launch_spmv32(const LevelDev &L, const float *x, float *y, cudaStream_t s);
 // One class launch of a Gauss-Seidel half sweep.  T = double (FP64 values and
 // vectors) or float (BF16 values, FP32 vectors); RT is the right-hand side type.

@@ -305,9 +305,13 @@ struct hpcgx_problem {
       note(launch_cg_p<double>(n, z, p, st, stream));
     }
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][2], stream, cudaEventRecordExternal));
+    // The mixed solver's FP64 SpMV derives its columns from the stencil
+    // offsets; the plain FP64 solver reads the int32 column arrays.
+    const bool implicit_cols = kind == G_MIXED;
     double spmv_bytes = 0.0;
     if (probe & HPCGX_PROBE_SPMV_FINE) {
-      // 12 B per real nonzero, x and y once, plus the fused p.Ap read of nothing extra
+      // 12 B (8 B without column reads) per real nonzero, x and y once; the
+      // fused p.Ap reads nothing extra
       int64_t nnz = 0;
       for (int s = 0; s < HPCGX_STENCIL; ++s) {
         const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
@@ -317,10 +321,10 @@ struct hpcgx_problem {
         for (int i = 0; i < L[0].nz; ++i) cz += (i + dz >= 0 && i + dz < L[0].nz);
         nnz += cx * cy * cz;
       }
-      spmv_bytes = 12.0 * nnz + 16.0 * n;
+      spmv_bytes = (implicit_cols ? 8.0 : 12.0) * nnz + 16.0 * n;
     }
     TRY(probed(HPCGX_PROBE_SPMV_FINE, spmv_bytes, [&]() {
-      return launch_spmv(L[0], p, Ap, &red, FIN_CG_PAP, st, done, stream);
+      return launch_spmv(L[0], p, Ap, &red, FIN_CG_PAP, st, done, stream, implicit_cols);
     }));
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][3], stream, cudaEventRecordExternal));
     note(launch_cg_xr(n, p, Ap, x, r, red, st, stream));
@@ -401,7 +405,7 @@ struct hpcgx_problem {
     // that the iteration graph never changes
     if (xu != x) CK(cudaMemcpyAsync(x, xu, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     CK(cudaMemcpyAsync(p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    note(launch_spmv(L[0], p, Ap, nullptr, 0, nullptr, nullptr, stream));
+    note(launch_spmv(L[0], p, Ap, nullptr, 0, nullptr, nullptr, stream, kind == G_MIXED));
     note(launch_cg_init(n, bu, Ap, r, red, st, stream));
     TRY(build_graph(kind));
     const bool per_iter = tol > 0.0 || probe != HPCGX_PROBE_NONE || times != nullptr;
@@ -792,6 +796,16 @@ int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
   p->note(launch_spmv(p->L[level], x, y, nullptr, 0, nullptr, nullptr, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  p->note(launch_spmv(p->L[level], x, y, nullptr, 0, nullptr, nullptr, p->stream, true));
   CK(cudaStreamSynchronize(p->stream));
   CK(cudaGetLastError());
   return HPCGX_OK;

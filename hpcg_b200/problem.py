@@ -135,10 +135,12 @@ class Problem:
         return b.value
 
     # ----------------------------------------------------------- operators
-    def spmv(self, x, level=0, y=None):
+    def spmv(self, x, level=0, y=None, stencil_cols=False):
+        """y = A x; stencil_cols derives the columns from the stencil offsets."""
         self._pre()
         y = self.empty(level) if y is None else y
-        check(lib().hpcgx_spmv(self.h, level, _ptr(x), _ptr(y)))
+        f = lib().hpcgx_spmv_stencil if stencil_cols else lib().hpcgx_spmv
+        check(f(self.h, level, _ptr(x), _ptr(y)))
         return y
 
     def symgs(self, r, x, level=0):

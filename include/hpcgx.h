@@ -92,6 +92,11 @@ int64_t hpcgx_rows(hpcgx_problem *p, int level);
 
 /* ComputeSPMV (src/ComputeSPMV.hpp:20): y = A_level x. */
 int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y);
+/* y = A_level x in FP64 with every column derived from the stencil offsets
+ * (row + offset) instead of read from the int32 column arrays: the outer SpMV
+ * of the mixed solver (no reference counterpart).  Loaded matrices are
+ * 27-point stencil matrices, so the sums are those of hpcgx_spmv. */
+int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y);
 /* ComputeSYMGS (src/ComputeSYMGS.hpp:20): one symmetric Gauss-Seidel sweep in
  * colour order (forward colours 0..7, backward 7..0), x updated in place. */
 int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x);

@@ -79,8 +79,12 @@ def test_spmv_bitexact(grid, oracle):
     L, b, xe, P = setup(grid, oracle)
     u, _, _ = seeded(oracle, L[0].nrow)
     for l, lev in enumerate(L):
+        want = oracle.spmv(lev, u[:lev.nrow])
         y = host(P.spmv(cuda(u[:lev.nrow]), level=l))
-        assert (y == oracle.spmv(lev, u[:lev.nrow])).all()
+        assert (y == want).all()
+        # columns from the stencil offsets (the mixed solver's outer SpMV)
+        y = host(P.spmv(cuda(u[:lev.nrow]), level=l, stencil_cols=True))
+        assert (y == want).all()
 
 
 def test_symgs_bitexact_colour_order(grid, oracle):
