@@ -29,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -55,10 +56,14 @@ def peaks():
 
 
 def model(dims, levels=4):
-    """HPCG's flop model (src/ReportResults.cpp:81-97) and the reference-style
-    byte model per iteration: SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n,
-    R+P 40 n_c, CG vectors 112 n (FP64); the mixed V-cycle moves 6 B/nnz (BF16
-    value + int32 column) and FP32 vectors."""
+    """HPCG's flop model (src/ReportResults.cpp:81-97) and the reference
+    implementation's bytes per iteration: SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n,
+    R+P 40 n_c, CG vectors 112 n (FP64; three dot products and three WAXPBYs of
+    src/CG.cpp:100-130); for the mixed solver the same steps with 6 B/nnz in the
+    V-cycle (BF16 value + int32 column) and FP32 vectors.  This design moves less
+    than either (restriction and prolongation inside the sweeps, zero-guess
+    sweeps, values-only BF16 matrix, columns from the stencil offsets), so the
+    effective bandwidths these models give exceed the HBM peak."""
     def nnz(nx, ny, nz):
         return (3 * nx - 2) * (3 * ny - 2) * (3 * nz - 2)
     lv = [(dims[0] >> l, dims[1] >> l, dims[2] >> l) for l in range(levels)]
@@ -284,6 +289,8 @@ def main():
     ap.add_argument("--grid", type=int, nargs="+", default=[512])
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--clocks-csv", default="",
+                    help="keep the nvidia-smi clock samples here (%%d = rank)")
     ap.add_argument("--ref-iters", type=int, default=0,
                     help="iterations the reference arm scales to (0: measured FP64 count)")
     ap.add_argument("--ref-sample", type=int, default=128)
@@ -355,8 +362,8 @@ def main():
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     iters_mixed = []
-    clk = Clocks(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                              else "", "bench_clocks_rank%d.csv" % rank))
+    clk = Clocks(args.clocks_csv % rank if args.clocks_csv else
+                 os.path.join(tempfile.gettempdir(), "hpcgx_bench_clocks_rank%d.csv" % rank))
     with clk:
         t0 = time.perf_counter()
         for i in range(args.steps):
@@ -456,10 +463,13 @@ def main():
                               "fp64_true": true_fp64},
         "x_rel_diff_vs_fp64": x_diff, "x_rel_err_vs_u": err_u,
         "gflops": {"mixed": gf_mixed, "fp64": gf_fp64, "model": "src/ReportResults.cpp:81-97"},
-        "hbm": {"mixed_gbs": hbm_mixed, "fp64_gbs": hbm_fp64, "mixed_frac": hbm_mixed / peak,
-                "fp64_frac": hbm_fp64 / peak, "peak_gbs": peak, "peak_kind": peak_kind},
-        "roofline": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f64>"),
-        "roofline_spmv": roofline(PROBE_SPMV_FINE, "k_spmv<double,double,1>"),
+        "hbm_effective": {"mixed_gbs": hbm_mixed, "fp64_gbs": hbm_fp64,
+                          "model": "bytes per iteration of the reference implementation's steps "
+                                   "(SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n, R+P 40 n_c, CG "
+                                   "vectors 112 n; mixed V-cycle 6 B/nnz and FP32 vectors) / time",
+                          "peak_gbs": peak, "peak_kind": peak_kind},
+        "roofline": roofline(PROBE_SPMV_FINE, "k_spmv<double,double,1,1>"),
+        "roofline_gs_bwd": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f64>"),
         "roofline_gs_fine_all_modes": roofline(PROBE_GS_FINE, "k_gs_class finest level, all modes"),
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8,
                 "d2h_bytes_per_step": n * 8},

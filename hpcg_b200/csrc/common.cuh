@@ -20,7 +20,10 @@
 //     (sz, sy, sx) order the reference generator emits
 //     (src/GenerateProblem_ref.cpp:152-172), which makes every row sum below
 //     round exactly as the reference's;
-//   * columns are int32 natural row indices; vectors stay in natural order.
+//   * columns are int32 natural row indices, read by the FP64 sweeps and the
+//     plain solver's SpMV; the mixed V-cycle and the mixed solver's FP64 SpMV
+//     derive them from the stencil offsets instead (row + offset), so the
+//     BF16 copy holds values only; vectors stay in natural order.
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>

@@ -8,8 +8,10 @@
 //     while they sit in L2;
 //   * a Gauss-Seidel half sweep is ONE launch per class: the two colours of a
 //     class only depend on each other along x inside a line, so a
-//     __syncthreads between them replaces a second launch (8 launches per
-//     symmetric sweep instead of 16);
+//     __syncthreads between them replaces a second launch; the last class's
+//     forward and backward half sweeps are one launch too (its last colour's
+//     backward update follows its forward update from registers), so a
+//     symmetric sweep is 7 launches instead of 16;
 //   * restriction (src/ComputeRestriction_ref.cpp:51) is fused into the last
 //     colour of the pre-smoother's backward sweep and prolongation
 //     (src/ComputeProlongation_ref.cpp:49) into the first colour of the

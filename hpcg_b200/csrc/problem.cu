@@ -2,9 +2,10 @@
 //
 // A problem owns one CUDA stream.  Matrix levels live in the colour-sorted
 // sliced-ELL layout described in common.cuh; CG keeps every scalar on the
-// device and runs each iteration as one CUDA graph (the V-cycle's 56 class
-// launches plus the 4 fused vector/SpMV kernels), so the host only reads the
-// residual norm when it has to test convergence.
+// device and runs each iteration as one CUDA graph (the V-cycle's 49 class
+// launches -- 7 per symmetric sweep, two sweeps on each of three levels and
+// one on the coarsest -- plus the 4 fused vector/SpMV kernels), so the host
+// only reads the residual norm when it has to test convergence.
 #include <cuda_runtime.h>
 
 #include <algorithm>
