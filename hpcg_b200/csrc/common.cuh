@@ -81,11 +81,10 @@ struct LevelMat {
   int nx, ny, nz;
   int64_t n;
   // Stencil offsets: slot s of row i holds column i + off[s] whenever the row
-  // has that neighbour (the layout enforces it when a level is loaded).  The
-  // mixed-precision V-cycle derives its columns from these instead of
-  // reading `cols` (slots without a neighbour hold value 0; their derived
-  // column is clamped into the matrix so that the multiplication by 0 reads
-  // valid memory).
+  // has that neighbour (the layout enforces it when a level is loaded), and
+  // column i with value 0 otherwise.  The mixed-precision V-cycle and the
+  // mixed solver's SpMV derive their columns from these instead of reading
+  // `cols`.
   int off[HPCGX_STENCIL];
 };
 

@@ -285,20 +285,36 @@ struct NeedAll {
 // Columns of storage row id derived from the stencil offsets, row + off[s] in
 // 32-bit arithmetic (vectors hold fewer than 2^31 rows).  Every level matrix
 // is a 27-point stencil matrix (the loaders reject any other pattern) whose
-// absent neighbours hold the value 0, so the stored int32 columns carry no
-// information: an interior row reads exactly row + off[s]; a row on the grid
-// boundary reads row + off[s] where that lies inside the vector and the row
-// itself elsewhere, and every slot that is not a neighbour multiplies by 0.
-template <class VT, class NEED>
+// absent neighbours hold the value 0 and the row itself as column, so the
+// stored int32 columns carry no information: an interior row reads exactly
+// row + off[s].  A slot of a boundary row without a neighbour multiplies its
+// x entry by 0.  EXACT takes the row itself for every such slot, as the
+// stored columns do: the Gauss-Seidel sweeps need it, since another block of
+// the same launch may write some rows for the first time (x there may hold
+// anything, NaN included) while this row's own entry is written already, and
+// it also keeps their gathers on lines the row reads anyway.  The SpMV reads
+// a fully written x, where any entry serves: it keeps row + off[s] where that
+// lies inside the vector and takes the row itself elsewhere (one compare per
+// slot, fewer instructions than the exact test).
+template <bool EXACT, class VT, class NEED>
 __device__ __forceinline__ void stencil_cols(const LevelMat<VT> &A, const RowId &id, NEED need,
                                              int32_t *col) {
   const int r32 = (int)id.row;
-  const bool inner = id.ix > 0 && id.ix + 1 < A.nx && id.iy > 0 && id.iy + 1 < A.ny &&
-                     id.iz > 0 && id.iz + 1 < A.nz;
-  if (inner) {
+  const bool xm = id.ix > 0, xp = id.ix + 1 < A.nx, ym = id.iy > 0, yp = id.iy + 1 < A.ny,
+             zm = id.iz > 0, zp = id.iz + 1 < A.nz;
+  if (xm && xp && ym && yp && zm && zp) {
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s)
       if (need(s)) col[s] = r32 + A.off[s];
+  } else if (EXACT) {
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s)
+      if (need(s)) {
+        const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
+        const bool nb = (dx < 0 ? xm : dx > 0 ? xp : true) && (dy < 0 ? ym : dy > 0 ? yp : true) &&
+                        (dz < 0 ? zm : dz > 0 ? zp : true);
+        col[s] = nb ? r32 + A.off[s] : r32;
+      }
   } else {
     const uint32_t n32 = (uint32_t)A.n;
 #pragma unroll
@@ -344,7 +360,7 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
         if (!IMPL) load_plane(A.cols, id.k, p, NeedAll(), col + 9 * p);
         load_plane(A.vals, id.k, p, NeedAll(), val + 9 * p);
       }
-      if (IMPL) stencil_cols(A, id, NeedAll(), col);
+      if (IMPL) stencil_cols<false>(A, id, NeedAll(), col);
       T xv[HPCGX_STENCIL];
 #pragma unroll
       for (int s = 0; s < HPCGX_STENCIL; ++s) xv[s] = __ldg(x + col[s]);
@@ -397,7 +413,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
     load_vals(A.vals, id.k, p, need, val + 9 * p);
     if (!IMPLICIT) load_plane(A.cols, id.k, p, need, col + 9 * p);
   }
-  if (IMPLICIT) stencil_cols(A, id, need, col);
+  if (IMPLICIT) stencil_cols<true>(A, id, need, col);
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
   if (PRO || RES) {
@@ -406,15 +422,16 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
   }
   T xi = ZERO ? T(0) : x[id.row];
   if (PRO) xi = rn_add(xi, __ldg(xc + crow));
-  // A slot without a neighbour holds value 0 (its column is the row itself,
-  // or, in the mixed V-cycle, a clamped derived column); in the zero-guess sweep
-  // x may be unwritten there, so its term -- a product with 0 -- is skipped.
+  // A slot without a neighbour holds value 0 and the row itself as column; in
+  // the zero-guess sweep x_i is unwritten, so that term -- a product with 0 --
+  // is skipped below.  The gather itself does not wait for the value: every
+  // column is in range.
   T xv[HPCGX_STENCIL];
 #pragma unroll
   for (int s = 0; s < HPCGX_STENCIL; ++s) {
     if (s == HPCGX_DIAG_SLOT) continue;
     if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
-    xv[s] = (ZERO && val[s] == T(0)) ? T(0) : x[col[s]];
+    xv[s] = x[col[s]];
   }
   T sum = rhs;
   const T d = val[HPCGX_DIAG_SLOT];
@@ -515,6 +532,9 @@ k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, 
     gs_row<ZERO, false, false, true>(A, row_of(C, A.nx, A.ny, 1, j0, t), 7, r, x,
                                      (const T *)nullptr, (T *)nullptr);
   __syncthreads();
+  // Colour 6 backward multiplies every slot; after a zero-guess forward part,
+  // rows of colours 6 and 7 in other blocks may still be unwritten, which the
+  // exact columns of slots without a neighbour never reach.
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
     gs_row<false, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
                                 (T *)nullptr);
