@@ -67,10 +67,21 @@ SIGNATURES = {
     "hpcgx_launch_count": (_I64, [_P]),
     "hpcgx_synchronize": (_I, [_P]),
     "hpcgx_set_stream": (_I, [_P, _P]),
+    "hpcgx_create_slab": (_I, [_I, _I, _I, _I, _I, _I, _I, C.POINTER(_P)]),
+    "hpcgx_nccl_unique_id": (_I, [_P, _I]),
+    "hpcgx_attach_nccl": (_I, [_P, _P, _I]),
+    "hpcgx_group_create": (_I, [_P, _I, C.POINTER(_P)]),
+    "hpcgx_group_destroy": (_I, [_P]),
+    "hpcgx_group_spmv": (_I, [_P, _I, _P, _P]),
+    "hpcgx_group_symgs": (_I, [_P, _I, _P, _P]),
+    "hpcgx_group_mg": (_I, [_P, _P, _P]),
+    "hpcgx_group_cg": (_I, [_P, _I, _P, _P, _I, _D, _IP, _DP, _DP]),
 }
 
 HPCGX_OK = 0
-ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ESTATE", 4: "ENONFINITE", 5: "ELAYOUT", 6: "ENOMEM"}
+ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ESTATE", 4: "ENONFINITE", 5: "ELAYOUT", 6: "ENOMEM",
+          7: "ECOMM"}
+NCCL_ID_BYTES = 128
 GEN_HPCG, GEN_VARCOEF = 0, 1
 PROBE_NONE, PROBE_GS_FINE, PROBE_SPMV_FINE, PROBE_GS_FINE_BWD = 0, 1, 2, 4
 CG_PLAIN, CG_MG, CG_MIXED = 0, 1, 2

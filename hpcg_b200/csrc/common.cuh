@@ -80,6 +80,10 @@ struct LevelMat {
   const int32_t *cols;
   int nx, ny, nz;
   int64_t n;
+  // z-slab halo planes present below / above (a neighbouring rank there), and
+  // the index range [lo, lo + span) of the vector including them
+  int zlo, zhi;
+  int lo, span;
   // Stencil offsets: slot s of row i holds column i + off[s] whenever the row
   // has that neighbour (the layout enforces it when a level is loaded), and
   // column i with value 0 otherwise.  The mixed-precision V-cycle and the

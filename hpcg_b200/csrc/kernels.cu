@@ -155,6 +155,34 @@ __device__ void finish(int fin, void *target, const double (&tot)[NV]) {
   }
 }
 
+// Applies the scalar step, or (sharded solve) stores this rank's totals for
+// the sum over the ranks that precedes it.
+template <int NV>
+__device__ void finish_or_defer(const Reduce &red, int fin, void *target, const double (&tot)[NV]) {
+  if (red.defer) {
+    for (int i = 0; i < NV; ++i) red.defer[i] = tot[i];
+    return;
+  }
+  finish<NV>(fin, target, tot);
+}
+
+template <int NV>
+__global__ void k_finish(int fin, const double *__restrict__ tot, CgState *st) {
+  double t[NV];
+  for (int i = 0; i < NV; ++i) t[i] = tot[i];
+  finish<NV>(fin, st, t);
+}
+
+// Sum over the ranks of an in-process group, in rank order, written back to
+// every rank's buffer.
+__global__ void k_rank_sum(int nranks, double *const *bufs, int count) {
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    double s = 0.0;
+    for (int r = 0; r < nranks; ++r) s += bufs[r][i];
+    for (int r = 0; r < nranks; ++r) bufs[r][i] = s;
+  }
+}
+
 // ---------------------------------------------------------------- geometry
 
 struct ClassSet {
@@ -325,7 +353,7 @@ __device__ __forceinline__ void stencil_cols(const LevelMat<VT> &A, const RowId 
                                              int32_t *col) {
   const int r32 = (int)id.row;
   const bool xm = id.ix > 0, xp = id.ix + 1 < A.nx, ym = id.iy > 0, yp = id.iy + 1 < A.ny,
-             zm = id.iz > 0, zp = id.iz + 1 < A.nz;
+             zm = id.iz > 0 || A.zlo, zp = id.iz + 1 < A.nz || A.zhi;
   if (xm && xp && ym && yp && zm && zp) {
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s)
@@ -340,12 +368,11 @@ __device__ __forceinline__ void stencil_cols(const LevelMat<VT> &A, const RowId 
         col[s] = nb ? r32 + A.off[s] : r32;
       }
   } else {
-    const uint32_t n32 = (uint32_t)A.n;
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s)
       if (need(s)) {
         const int cc = r32 + A.off[s];
-        col[s] = (uint32_t)cc < n32 ? cc : r32;
+        col[s] = (uint32_t)(cc - A.lo) < (uint32_t)A.span ? cc : r32;
       }
   }
 }
@@ -397,7 +424,8 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
   }
   if (DOT) {
     double v[1] = {acc}, tot[1];
-    if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(fin, fin_target, tot);
+    if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0)
+      finish_or_defer<1>(red, fin, fin_target, tot);
   }
 }
 
@@ -563,6 +591,60 @@ k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, 
                                 (T *)nullptr);
 }
 
+// Residual restricted at the injected points (colour 0: even ix, iy, iz):
+// rc = rf - (A x) there, (A x)_i summed over the slots from 0 in order as
+// ComputeSPMV_ref does (src/ComputeSPMV_ref.cpp:64-70), then
+// src/ComputeRestriction_ref.cpp:51.  The standalone form of GS_RESTRICT, for
+// the sharded V-cycle, where the halo of x is exchanged between the sweep and
+// the residual (src/ComputeMG_ref.cpp:49-51).
+template <class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads)
+k_restrict_residual(LevelMat<VT> A, ClassInfo C0, int64_t nc, const RT *__restrict__ rf,
+                    const T *__restrict__ x, T *__restrict__ rc, const int *__restrict__ done) {
+  if (done && *done) return;
+  constexpr bool IMPLICIT = std::is_same<VT, uint16_t>::value;
+  const int nxc = A.nx >> 1, nyc = A.ny >> 1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int ixc = (int)(i % nxc), iyc = (int)((i / nxc) % nyc);
+    const int izc = (int)(i / ((int64_t)nxc * nyc));
+    RowId id;
+    id.ix = 2 * ixc;
+    id.iy = 2 * iyc;
+    id.iz = 2 * izc;
+    id.row = ((int64_t)id.iz * A.ny + id.iy) * A.nx + id.ix;
+    id.k = C0.start[0] + ((int64_t)izc * C0.nyq + iyc) * C0.len[0] + ixc;  // colour 0
+    int32_t col[HPCGX_STENCIL];
+    T val[HPCGX_STENCIL];
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      load_vals(A.vals, id.k, p, NeedAll(), val + 9 * p);
+      if (!IMPLICIT) load_plane(A.cols, id.k, p, NeedAll(), col + 9 * p);
+    }
+    if (IMPLICIT) stencil_cols<true>(A, id, NeedAll(), col);
+    T ax = T(0);
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s) ax = rn_add(ax, rn_mul(val[s], x[col[s]]));
+    rc[i] = rn_sub(vec_to(__ldg(rf + id.row), T()), ax);
+  }
+}
+
+// xf += xc at the injected points (src/ComputeProlongation_ref.cpp:49), in the
+// vector type of the V-cycle.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+k_prolong(int64_t nc, int nxf, int nyf, const T *__restrict__ xc, T *xf,
+          const int *__restrict__ done) {
+  if (done && *done) return;
+  const int nxc = nxf >> 1, nyc = nyf >> 1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nc;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ixc = i % nxc, iyc = (i / nxc) % nyc, izc = i / ((int64_t)nxc * nyc);
+    const int64_t f = ((2 * izc) * nyf + 2 * iyc) * nxf + 2 * ixc;
+    xf[f] = rn_add(xf[f], xc[i]);
+  }
+}
+
 // ---------------------------------------------------------------- vectors
 
 __global__ void __launch_bounds__(kThreads)
@@ -639,10 +721,11 @@ __global__ void k_copy(int64_t n, const double *__restrict__ x, double *y,
     y[i] = x[i];
 }
 
-__global__ void k_fill_uniform(int64_t n, uint64_t seed, double lo, double hi, double *v) {
+__global__ void k_fill_uniform(int64_t n, uint64_t seed, uint64_t offset, double lo, double hi,
+                               double *v) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
-    v[i] = rn_add(lo, rn_mul(rn_sub(hi, lo), uniform01(seed, (uint64_t)i)));
+    v[i] = rn_add(lo, rn_mul(rn_sub(hi, lo), uniform01(seed, offset + (uint64_t)i)));
 }
 
 __device__ __forceinline__ double normal01(uint64_t seed, uint64_t i) {
@@ -671,7 +754,8 @@ k_cg_init(int64_t n, const double *__restrict__ b, const double *__restrict__ Ap
     acc += ri * ri;
   }
   double v[1] = {acc}, tot[1];
-  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(FIN_CG_INIT, st, tot);
+  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0)
+    finish_or_defer<1>(red, FIN_CG_INIT, st, tot);
 }
 
 // rtz = r.z (src/CG.cpp:109/112); for the flexible solver also z.Ap_{k-1}.
@@ -690,10 +774,12 @@ k_cg_rz(int64_t n, const double *__restrict__ r, const ZT *__restrict__ z,
   }
   if (FLEX) {
     double v[2] = {a0, a1}, tot[2];
-    if (grid_reduce<2>(v, red, tot) && threadIdx.x == 0) finish<2>(FIN_CG_RZ, st, tot);
+    if (grid_reduce<2>(v, red, tot) && threadIdx.x == 0)
+      finish_or_defer<2>(red, FIN_CG_RZ, st, tot);
   } else {
     double v[1] = {a0}, tot[1];
-    if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(FIN_CG_RZ, st, tot);
+    if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0)
+      finish_or_defer<1>(red, FIN_CG_RZ, st, tot);
   }
 }
 
@@ -726,7 +812,8 @@ k_cg_xr(int64_t n, const double *__restrict__ p, const double *__restrict__ Ap, 
     acc += ri * ri;
   }
   double v[1] = {acc}, tot[1];
-  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish<1>(FIN_CG_RR, st, tot);
+  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0)
+    finish_or_defer<1>(red, FIN_CG_RR, st, tot);
 }
 
 __global__ void k_copy_z(int64_t n, const double *__restrict__ r, double *z,
@@ -741,6 +828,7 @@ __global__ void k_copy_z(int64_t n, const double *__restrict__ r, double *z,
 
 struct Geo {
   int nx, ny, nz;
+  int zlo, zhi;   // z-slab: the planes below / above belong to a neighbouring rank
   int64_t cstart[8], ccount[8];
   int len[2];
   int nyq[4];
@@ -779,7 +867,8 @@ __device__ __forceinline__ bool neighbour(const Geo &g, int ix, int iy, int iz, 
                                           int64_t row, int64_t &col) {
   const int dx = s % 3 - 1, dy = (s / 3) % 3 - 1, dz = s / 9 - 1;
   const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
-  if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) return false;
+  if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny) return false;
+  if ((jz < 0 && !g.zlo) || (jz >= g.nz && !g.zhi)) return false;
   col = row + (int64_t)dz * g.nx * g.ny + (int64_t)dy * g.nx + dx;
   return true;
 }
@@ -956,6 +1045,8 @@ Geo geo_of(const LevelDev &L) {
   g.nx = L.nx;
   g.ny = L.ny;
   g.nz = L.nz;
+  g.zlo = L.zlo;
+  g.zhi = L.zhi;
   for (int c = 0; c < 8; ++c) {
     g.cstart[c] = L.cstart[c];
     g.ccount[c] = L.ccount[c];
@@ -982,6 +1073,10 @@ LevelMat<VT> mat_of(const LevelDev &L, const VT *vals) {
   A.ny = L.ny;
   A.nz = L.nz;
   A.n = L.n;
+  A.zlo = L.zlo;
+  A.zhi = L.zhi;
+  A.lo = L.zlo ? -L.nx * L.ny : 0;
+  A.span = (int)L.n - A.lo + (L.zhi ? L.nx * L.ny : 0);
   return A;
 }
 
@@ -1183,6 +1278,49 @@ int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *
   return 1;
 }
 
+template <class T, class RT>
+int launch_restrict_residual(const LevelDev &F, const RT *rf, const T *xf, T *rc, const int *done,
+                             cudaStream_t s) {
+  const int64_t nc = (int64_t)(F.nx / 2) * (F.ny / 2) * (F.nz / 2);
+  if (nc == 0) return 0;
+  k_restrict_residual<<<grid_for(nc), kThreads, 0, s>>>(mat_of(F, ValsOf<T>::get(F)), F.cls[0],
+                                                        nc, rf, xf, rc, done);
+  return 1;
+}
+template int launch_restrict_residual<double, double>(const LevelDev &, const double *,
+                                                      const double *, double *, const int *,
+                                                      cudaStream_t);
+template int launch_restrict_residual<float, double>(const LevelDev &, const double *,
+                                                     const float *, float *, const int *,
+                                                     cudaStream_t);
+template int launch_restrict_residual<float, float>(const LevelDev &, const float *, const float *,
+                                                    float *, const int *, cudaStream_t);
+
+template <class T>
+int launch_prolong(const LevelDev &F, int64_t nc, const T *xc, T *xf, const int *done,
+                   cudaStream_t s) {
+  if (nc == 0) return 0;
+  k_prolong<T><<<grid_for(nc), kThreads, 0, s>>>(nc, F.nx, F.ny, xc, xf, done);
+  return 1;
+}
+template int launch_prolong<double>(const LevelDev &, int64_t, const double *, double *,
+                                    const int *, cudaStream_t);
+template int launch_prolong<float>(const LevelDev &, int64_t, const float *, float *, const int *,
+                                   cudaStream_t);
+
+int launch_finish(int fin, int nv, const double *tot, CgState *st, cudaStream_t s) {
+  if (nv == 2)
+    k_finish<2><<<1, 1, 0, s>>>(fin, tot, st);
+  else
+    k_finish<1><<<1, 1, 0, s>>>(fin, tot, st);
+  return 1;
+}
+
+int launch_rank_sum(int nranks, double *const *bufs, int count, cudaStream_t s) {
+  k_rank_sum<<<1, 32, 0, s>>>(nranks, bufs, count);
+  return 1;
+}
+
 template int launch_gs_class<double, double>(const LevelDev &, int, int, int, const double *,
                                              double *, const double *, double *, const int *,
                                              cudaStream_t);
@@ -1228,9 +1366,9 @@ int launch_copy(int64_t n, const double *x, double *y, const int *done, cudaStre
   return 1;
 }
 
-int launch_fill_uniform(int64_t n, uint64_t seed, double lo, double hi, double *v,
+int launch_fill_uniform(int64_t n, uint64_t seed, uint64_t offset, double lo, double hi, double *v,
                         cudaStream_t s) {
-  k_fill_uniform<<<grid_for(n), kThreads, 0, s>>>(n, seed, lo, hi, v);
+  k_fill_uniform<<<grid_for(n), kThreads, 0, s>>>(n, seed, offset, lo, hi, v);
   return 1;
 }
 

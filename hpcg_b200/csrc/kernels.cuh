@@ -13,6 +13,10 @@ struct LevelDev {
   ClassInfo cls[4] = {};
   int lines_per_block[4] = {}, blocks[4] = {}, threads[4] = {};
   int spmv_blocks = 0;        // all four classes in one launch
+  // z-slab of a sharded problem: a neighbouring rank owns the plane below
+  // (zlo) / above (zhi); vectors read by SpMV and Gauss-Seidel then hold one
+  // halo plane on each side (indices -nx*ny..-1 and n..n+nx*ny-1)
+  int zlo = 0, zhi = 0;
   double *vals = nullptr;     // storage_rows*27, FP64
   int32_t *cols = nullptr;    // storage_rows*27
   uint16_t *vals16 = nullptr; // storage_rows*27, BF16 (mixed precision)
@@ -40,6 +44,10 @@ struct Reduce {
   double *partials = nullptr;
   unsigned int *counter = nullptr;
   int64_t capacity = 0;       // doubles in partials
+  // Sharded solve: the last block stores this rank's totals here instead of
+  // applying the scalar step, which launch_finish applies after the totals
+  // were summed over the ranks.
+  double *defer = nullptr;
 };
 
 // Which scalar a finished reduction updates.
@@ -98,13 +106,28 @@ int launch_restriction(int64_t nc, const LevelDev &F, const double *rf, const do
 int launch_prolongation(int64_t nc, const LevelDev &F, const double *xc, double *xf,
                          cudaStream_t s);
 int launch_copy(int64_t n, const double *x, double *y, const int *done, cudaStream_t s);
-int launch_fill_uniform(int64_t n, uint64_t seed, double lo, double hi, double *v,
-                         cudaStream_t s);
+int launch_fill_uniform(int64_t n, uint64_t seed, uint64_t offset, double lo, double hi,
+                         double *v, cudaStream_t s);
 int launch_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double *v, cudaStream_t s);
 
 // CG pieces ---------------------------------------------------------------
 int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, const Reduce &red,
                     CgState *st, cudaStream_t s);
+// The scalar step `fin` on nv totals (a deferred reduction, summed over ranks).
+int launch_finish(int fin, int nv, const double *tot, CgState *st, cudaStream_t s);
+// bufs: device array of nranks pointers to `count` doubles each; every buffer
+// receives the sum over the ranks, taken in rank order.
+int launch_rank_sum(int nranks, double *const *bufs, int count, cudaStream_t s);
+// Standalone restriction of the residual at the injected points,
+// rc = rf - (A x) there (src/ComputeSPMV_ref.cpp + src/ComputeRestriction_ref.cpp:51),
+// and prolongation xf += xc at the injected points; used where a halo
+// exchange separates them from the sweeps.
+template <class T, class RT>
+int launch_restrict_residual(const LevelDev &F, const RT *rf, const T *xf, T *rc, const int *done,
+                             cudaStream_t s);
+template <class T>
+int launch_prolong(const LevelDev &F, int64_t nc, const T *xc, T *xf, const int *done,
+                   cudaStream_t s);
 template <class ZT>
 int launch_cg_rz(int64_t n, const double *r, const ZT *z, const double *Ap, const Reduce &red,
                   CgState *st, cudaStream_t s);

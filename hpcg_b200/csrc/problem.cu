@@ -7,6 +7,8 @@
 // one on the coarsest -- plus the 4 fused vector/SpMV kernels), so the host
 // only reads the residual norm when it has to test convergence.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nccl.h>
 
 #include <algorithm>
 #include <memory>
@@ -17,6 +19,8 @@
 #include <string>
 #include <thread>
 #include <type_traits>
+#include <functional>
+#include <mutex>
 #include <vector>
 
 #include "../../include/hpcgx.h"
@@ -68,6 +72,18 @@ inline float *lvl_r(LevelDev &A, float *) { return A.r32; }
 
 enum GraphKind { G_FP64_PREC = 0, G_FP64_NOPREC = 1, G_MIXED = 2, G_COUNT = 3 };
 
+// One step of a sharded operation (see hpcgx_problem::add*).
+enum StepKind { STEP_LAUNCH = 0, STEP_HALO = 1, STEP_SUM = 2 };
+struct Step {
+  int kind = STEP_LAUNCH;
+  std::function<int()> launch;   // STEP_LAUNCH: enqueue on the problem's stream
+  int level = 0;                 // STEP_HALO: level vector vec of esize-byte elements
+  void *vec = nullptr;
+  int esize = 0;
+  int fin = -1, nv = 0;          // STEP_SUM: nv totals in gsum, then scalar step fin
+};
+using Plan = std::vector<Step>;
+
 struct Probe {
   cudaEvent_t a, b;
   double bytes;
@@ -117,6 +133,16 @@ struct hpcgx_problem {
   double probe_ms[3] = {}, probe_bytes[3] = {};
   int64_t probe_launches[3] = {};
   size_t bytes = 0;
+  // vectors that SpMV / Gauss-Seidel read as x carry one halo plane below and
+  // above (zero unless a neighbouring rank fills them); their allocations
+  std::vector<void *> halo_bases;
+  // ---- sharding: this problem is z-slab `rank` of `nranks`; the global grid
+  // is nx x ny x (nz nranks) (src/GenerateGeometry.cpp with npx = npy = 1)
+  int nranks = 1, rank = 0;
+  struct NcclLink *nccl = nullptr;   // exchange backend, one process per GPU
+  double *gsum = nullptr;            // this rank's deferred reduction totals
+  double *hstage[kMaxLevels] = {};   // haloed FP64 staging of operator inputs
+  bool sharded() const { return nranks > 1 || nccl != nullptr; }
 
   ~hpcgx_problem();
   int alloc(void **ptr, size_t n) {
@@ -127,6 +153,16 @@ struct hpcgx_problem {
                                     cudaGetErrorString(e));
     }
     bytes += n;
+    return HPCGX_OK;
+  }
+  // n elements of esize bytes with one zeroed halo plane (plane elements) on
+  // each side; *ptr points at element 0.
+  int alloc_halo(void **ptr, int64_t n, size_t esize, int64_t plane) {
+    void *base = nullptr;
+    TRY(alloc(&base, (size_t)(n + 2 * plane) * esize));
+    halo_bases.push_back(base);
+    CK(cudaMemset(base, 0, (size_t)(n + 2 * plane) * esize));
+    *ptr = static_cast<char *>(base) + plane * esize;
     return HPCGX_OK;
   }
   void note(int launched) { launches += launched; }
@@ -449,10 +485,234 @@ struct hpcgx_problem {
     if (h.nonfinite) return fail(HPCGX_ENONFINITE, "CG: residual norm is not finite");
     return HPCGX_OK;
   }
+
+  // ---- sharded operations as step lists
+  // The steps of one operation on this rank: kernel launches, halo exchanges
+  // of a level vector (src/ExchangeHalo.cpp:34-110) and sums over the ranks of
+  // the deferred reduction totals followed by their scalar step (the
+  // MPI_Allreduce of src/ComputeDotProduct_ref.cpp:66-77).  Every rank plans
+  // the same sequence; a runner executes it over NCCL or in-process.
+  Reduce deferred() const {
+    Reduce d = red;
+    d.defer = gsum;
+    return d;
+  }
+  void add(Plan &pl, std::function<int()> f) {
+    Step s;
+    s.kind = STEP_LAUNCH;
+    s.launch = std::move(f);
+    pl.push_back(std::move(s));
+  }
+  void add_halo(Plan &pl, int l, void *v, int esize) {
+    Step s;
+    s.kind = STEP_HALO;
+    s.level = l;
+    s.vec = v;
+    s.esize = esize;
+    pl.push_back(std::move(s));
+  }
+  void add_sum(Plan &pl, int fin, int nv) {
+    Step s;
+    s.kind = STEP_SUM;
+    s.fin = fin;
+    s.nv = nv;
+    pl.push_back(std::move(s));
+  }
+  // The halo planes of x read as zero (the first sweep after ZeroVector:
+  // ExchangeHalo of a zero vector, src/ComputeMG_ref.cpp:42 + src/ComputeSYMGS_ref.cpp:56).
+  template <class T>
+  int zero_halo(int l, T *x) {
+    const LevelDev &A = L[l];
+    const int64_t plane = (int64_t)A.nx * A.ny;
+    if (A.zlo) CK(cudaMemsetAsync(x - plane, 0, plane * sizeof(T), stream));
+    if (A.zhi) CK(cudaMemsetAsync(x + A.n, 0, plane * sizeof(T), stream));
+    return HPCGX_OK;
+  }
+  // One symmetric sweep of level l (7 class launches) after the halo of x.
+  template <class T, class RT>
+  void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done) {
+    const int m0 = zero ? GS_ZERO_GUESS : GS_PLAIN;
+    for (int q = 0; q < 3; ++q)
+      add(pl, [=]() {
+        note(launch_gs_class<T, RT>(L[l], q, 0, m0, r, x, nullptr, nullptr, done, stream));
+        return HPCGX_OK;
+      });
+    add(pl, [=]() {
+      note(launch_gs_class<T, RT>(L[l], 3, 0, GS_SYM3 | m0, r, x, nullptr, nullptr, done, stream));
+      return HPCGX_OK;
+    });
+    for (int q = 2; q >= 0; --q)
+      add(pl, [=]() {
+        note(launch_gs_class<T, RT>(L[l], q, 1, GS_PLAIN, r, x, nullptr, nullptr, done, stream));
+        return HPCGX_OK;
+      });
+  }
+  // The V-cycle of src/ComputeMG_ref.cpp:39-63 on a z-slab: restriction and
+  // prolongation are separate launches, since the reference exchanges the
+  // halo of x between the pre-smoother and the residual and between the
+  // prolongation and the post-smoother.  x0 must be a haloed vector.
+  template <class T, class RT0>
+  void plan_vcycle(Plan &pl, const RT0 *r0, T *x0, const int *done) {
+    T *xl[kMaxLevels];
+    for (int l = 0; l < nlev; ++l) xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
+    auto rl = [&](int l) { return lvl_r(L[l], (T *)nullptr); };
+    for (int l = 0; l + 1 < nlev; ++l) {
+      T *x = xl[l];
+      add(pl, [=]() { return zero_halo<T>(l, x); });
+      if (l == 0)
+        plan_sweeps<T, RT0>(pl, 0, r0, x, true, done);
+      else
+        plan_sweeps<T, T>(pl, l, rl(l), x, true, done);
+      add_halo(pl, l, x, sizeof(T));
+      T *rc = rl(l + 1);
+      if (l == 0)
+        add(pl, [=]() {
+          note(launch_restrict_residual<T, RT0>(L[0], r0, x, rc, done, stream));
+          return HPCGX_OK;
+        });
+      else {
+        const T *rf = rl(l);
+        add(pl, [=]() {
+          note(launch_restrict_residual<T, T>(L[l], rf, x, rc, done, stream));
+          return HPCGX_OK;
+        });
+      }
+    }
+    const int c = nlev - 1;
+    {
+      T *x = xl[c];
+      add(pl, [=]() { return zero_halo<T>(c, x); });
+      if (c == 0)
+        plan_sweeps<T, RT0>(pl, 0, r0, x, true, done);
+      else
+        plan_sweeps<T, T>(pl, c, rl(c), x, true, done);
+    }
+    for (int l = nlev - 2; l >= 0; --l) {
+      T *x = xl[l];
+      const T *xc = xl[l + 1];
+      const int64_t nc = L[l + 1].n;
+      add(pl, [=]() {
+        note(launch_prolong<T>(L[l], nc, xc, x, done, stream));
+        return HPCGX_OK;
+      });
+      add_halo(pl, l, x, sizeof(T));
+      if (l == 0)
+        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done);
+      else
+        plan_sweeps<T, T>(pl, l, rl(l), x, false, done);
+    }
+  }
+  // The haloed staging vector of level l (operator inputs arrive without halo).
+  int staging_halo(int l, double **out) {
+    if (!hstage[l]) {
+      const int64_t plane = (int64_t)L[l].nx * L[l].ny;
+      TRY(alloc_halo((void **)&hstage[l], L[l].n, sizeof(double), plane));
+    }
+    *out = hstage[l];
+    return HPCGX_OK;
+  }
+  void plan_copy(Plan &pl, const double *from, double *to, int64_t n) {
+    add(pl, [=]() {
+      CK(cudaMemcpyAsync(to, from, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+      return HPCGX_OK;
+    });
+  }
+  int plan_spmv(Plan &pl, int l, const double *x, double *y) {
+    double *xs = nullptr;
+    TRY(staging_halo(l, &xs));
+    plan_copy(pl, x, xs, L[l].n);
+    add_halo(pl, l, xs, sizeof(double));
+    add(pl, [=]() {
+      note(launch_spmv(L[l], xs, y, nullptr, 0, nullptr, nullptr, stream));
+      return HPCGX_OK;
+    });
+    return HPCGX_OK;
+  }
+  int plan_symgs(Plan &pl, int l, const double *r, double *x) {
+    double *xs = nullptr;
+    TRY(staging_halo(l, &xs));
+    plan_copy(pl, x, xs, L[l].n);
+    add_halo(pl, l, xs, sizeof(double));   // src/ComputeSYMGS_ref.cpp:56
+    plan_sweeps<double, double>(pl, l, r, xs, false, nullptr);
+    plan_copy(pl, xs, x, L[l].n);
+    return HPCGX_OK;
+  }
+  int plan_mg(Plan &pl, const double *r, double *x) {
+    double *xs = nullptr;
+    TRY(staging_halo(0, &xs));
+    plan_vcycle<double, double>(pl, r, xs, nullptr);
+    plan_copy(pl, xs, x, L[0].n);
+    return HPCGX_OK;
+  }
+  // CG set-up (src/CG.cpp:86-92): p = x, Ap = A p, r = b - Ap, normr0.
+  void plan_cg_init(Plan &pl, int kind, const double *bu) {
+    const int64_t n = L[0].n;
+    add(pl, [=]() {
+      CK(cudaMemcpyAsync(p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+      return HPCGX_OK;
+    });
+    add_halo(pl, 0, p, sizeof(double));
+    add(pl, [=]() {
+      note(launch_spmv(L[0], p, Ap, nullptr, 0, nullptr, nullptr, stream, kind == G_MIXED));
+      return HPCGX_OK;
+    });
+    add(pl, [=]() {
+      note(launch_cg_init(n, bu, Ap, r, deferred(), st, stream));
+      return HPCGX_OK;
+    });
+    add_sum(pl, FIN_CG_INIT, 1);
+  }
+  // One CG iteration (src/CG.cpp:100-130): the fused kernels of the one-GPU
+  // iteration with every reduction summed over the ranks before its scalar step.
+  void plan_cg_iteration(Plan &pl, int kind) {
+    const int64_t n = L[0].n;
+    const int *done = &st->done;
+    if (kind == G_FP64_NOPREC)
+      add(pl, [=]() {
+        note(launch_copy_z(n, r, z, st, stream));
+        return HPCGX_OK;
+      });
+    else if (kind == G_FP64_PREC)
+      plan_vcycle<double, double>(pl, r, z, done);
+    else
+      plan_vcycle<float, double>(pl, r, z32, done);
+    const bool mixed = kind == G_MIXED;
+    add(pl, [=]() {
+      if (mixed) {
+        note(launch_cg_rz<float>(n, r, z32, Ap, deferred(), st, stream));
+      } else {
+        note(launch_cg_rz<double>(n, r, z, nullptr, deferred(), st, stream));
+      }
+      return HPCGX_OK;
+    });
+    add_sum(pl, FIN_CG_RZ, mixed ? 2 : 1);
+    add(pl, [=]() {
+      if (mixed)
+        note(launch_cg_p<float>(n, z32, p, st, stream));
+      else
+        note(launch_cg_p<double>(n, z, p, st, stream));
+      return HPCGX_OK;
+    });
+    add_halo(pl, 0, p, sizeof(double));
+    add(pl, [=]() {
+      const Reduce d = deferred();
+      note(launch_spmv(L[0], p, Ap, &d, FIN_CG_PAP, st, done, stream, mixed));
+      return HPCGX_OK;
+    });
+    add_sum(pl, FIN_CG_PAP, 1);
+    add(pl, [=]() {
+      note(launch_cg_xr(n, p, Ap, x, r, deferred(), st, stream));
+      return HPCGX_OK;
+    });
+    add_sum(pl, FIN_CG_RR, 1);
+  }
 };
+
+void nccl_release(NcclLink *link);
 
 hpcgx_problem::~hpcgx_problem() {
   cudaSetDevice(device);
+  if (nccl) nccl_release(nccl);
   if (stream) cudaStreamSynchronize(stream);
   for (auto &pr : event_pool) {
     cudaEventDestroy(pr.a);
@@ -468,14 +728,12 @@ hpcgx_problem::~hpcgx_problem() {
     cudaFree(L[l].cols);
     cudaFree(L[l].vals16);
     cudaFree(L[l].r64);
-    cudaFree(L[l].x64);
     cudaFree(L[l].r32);
-    cudaFree(L[l].x32);
   }
   for (double *ptr : stage) cudaFree(ptr);
-  for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)z, (void *)p, (void *)Ap,
-                    (void *)z32, (void *)tmp, (void *)result, (void *)st,
-                    (void *)red.partials, (void *)red.counter})
+  for (void *ptr : halo_bases) cudaFree(ptr);
+  for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)Ap, (void *)tmp, (void *)result,
+                    (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter})
     cudaFree(ptr);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -604,6 +862,248 @@ int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
 
 }  // namespace
 
+// ======================================================================
+// Sharding backends.
+//
+// NCCL is opened at run time -- the library torch.distributed already loaded
+// when there is one, else the system's -- so single-GPU users of libhpcgx need
+// no NCCL; only the types come from nccl.h.
+struct NcclApi {
+  ncclResult_t (*GetUniqueId)(ncclUniqueId *) = nullptr;
+  ncclResult_t (*CommInitRank)(ncclComm_t *, int, ncclUniqueId, int) = nullptr;
+  ncclResult_t (*CommDestroy)(ncclComm_t) = nullptr;
+  ncclResult_t (*Send)(const void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*Recv)(void *, size_t, ncclDataType_t, int, ncclComm_t, cudaStream_t) = nullptr;
+  ncclResult_t (*AllReduce)(const void *, void *, size_t, ncclDataType_t, ncclRedOp_t, ncclComm_t,
+                            cudaStream_t) = nullptr;
+  ncclResult_t (*GroupStart)() = nullptr;
+  ncclResult_t (*GroupEnd)() = nullptr;
+  const char *(*GetErrorString)(ncclResult_t) = nullptr;
+};
+
+static NcclApi *nccl_api() {
+  static NcclApi api;
+  static bool ok = false;
+  static std::once_flag once;
+  std::call_once(once, []() {
+    void *h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+    if (!h) return;
+    api.GetUniqueId = (decltype(api.GetUniqueId))dlsym(h, "ncclGetUniqueId");
+    api.CommInitRank = (decltype(api.CommInitRank))dlsym(h, "ncclCommInitRank");
+    api.CommDestroy = (decltype(api.CommDestroy))dlsym(h, "ncclCommDestroy");
+    api.Send = (decltype(api.Send))dlsym(h, "ncclSend");
+    api.Recv = (decltype(api.Recv))dlsym(h, "ncclRecv");
+    api.AllReduce = (decltype(api.AllReduce))dlsym(h, "ncclAllReduce");
+    api.GroupStart = (decltype(api.GroupStart))dlsym(h, "ncclGroupStart");
+    api.GroupEnd = (decltype(api.GroupEnd))dlsym(h, "ncclGroupEnd");
+    api.GetErrorString = (decltype(api.GetErrorString))dlsym(h, "ncclGetErrorString");
+    ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.Send && api.Recv &&
+         api.AllReduce && api.GroupStart && api.GroupEnd && api.GetErrorString;
+  });
+  return ok ? &api : nullptr;
+}
+
+#define NCCLCK(call)                                                                  \
+  do {                                                                                \
+    ncclResult_t r_ = (call);                                                         \
+    if (r_ != ncclSuccess)                                                            \
+      return fail(HPCGX_ECOMM, std::string(#call) + ": " + nccl_api()->GetErrorString(r_)); \
+  } while (0)
+
+struct NcclLink {
+  ncclComm_t comm = nullptr;
+};
+
+void nccl_release(NcclLink *link) {
+  if (link->comm && nccl_api()) nccl_api()->CommDestroy(link->comm);
+  delete link;
+}
+
+namespace {
+
+// Halo exchange of one level vector of a z-slab over NCCL: this rank's first
+// plane to the rank below (its upper halo), its last plane to the rank above
+// (its lower halo), and the converse into this rank's halo planes.
+int nccl_halo(hpcgx_problem *p, int l, void *v, int esize) {
+  const LevelDev &A = p->L[l];
+  if (!A.zlo && !A.zhi) return HPCGX_OK;
+  NcclApi *api = nccl_api();
+  const size_t plane = (size_t)A.nx * A.ny;
+  const ncclDataType_t t = esize == 8 ? ncclFloat64 : ncclFloat32;
+  char *b = static_cast<char *>(v);
+  ncclComm_t c = p->nccl->comm;
+  NCCLCK(api->GroupStart());
+  if (A.zlo) {
+    NCCLCK(api->Send(b, plane, t, p->rank - 1, c, p->stream));
+    NCCLCK(api->Recv(b - plane * esize, plane, t, p->rank - 1, c, p->stream));
+  }
+  if (A.zhi) {
+    NCCLCK(api->Send(b + (A.n - (int64_t)plane) * esize, plane, t, p->rank + 1, c, p->stream));
+    NCCLCK(api->Recv(b + A.n * esize, plane, t, p->rank + 1, c, p->stream));
+  }
+  NCCLCK(api->GroupEnd());
+  return HPCGX_OK;
+}
+
+// Runs one rank's plan: halo steps over NCCL, sums as an all-reduce of the
+// deferred totals.  Without a communicator (one rank) both are no-ops.
+int run_plan(hpcgx_problem *p, Plan &pl) {
+  for (Step &s : pl) {
+    if (s.kind == STEP_LAUNCH) {
+      TRY(s.launch());
+    } else if (s.kind == STEP_HALO) {
+      if (p->nccl) TRY(nccl_halo(p, s.level, s.vec, s.esize));
+    } else {
+      if (p->nccl)
+        NCCLCK(nccl_api()->AllReduce(p->gsum, p->gsum, s.nv, ncclFloat64, ncclSum, p->nccl->comm,
+                                     p->stream));
+      if (s.fin >= 0) p->note(launch_finish(s.fin, s.nv, p->gsum, p->st, p->stream));
+    }
+  }
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+}  // namespace
+
+// Every rank of a z-slab decomposition held by one process on one GPU and one
+// stream: the ranks' plans run step by step in lockstep, halo steps become
+// device copies between the ranks' vectors and sums add the ranks' totals in
+// rank order.  It runs the multi-rank algorithm on a single GPU (tests,
+// emulation) without kernels that wait on each other.
+struct hpcgx_group {
+  std::vector<hpcgx_problem *> ranks;
+  std::vector<cudaStream_t> saved;   // each rank's stream before the group
+  double **bufs = nullptr;           // device array of every rank's gsum
+  ~hpcgx_group() {
+    if (bufs) cudaFree(bufs);
+  }
+};
+
+namespace {
+
+using Runner = std::function<int(std::vector<Plan> &)>;
+
+int group_run(hpcgx_group *g, std::vector<Plan> &plans) {
+  const int P = (int)g->ranks.size();
+  const size_t ns = plans[0].size();
+  for (const Plan &pl : plans)
+    if (pl.size() != ns) return fail(HPCGX_ESTATE, "ranks planned different step sequences");
+  hpcgx_problem *p0 = g->ranks[0];
+  cudaStream_t s = p0->stream;
+  for (size_t i = 0; i < ns; ++i) {
+    const Step &s0 = plans[0][i];
+    for (int r = 1; r < P; ++r)
+      if (plans[r][i].kind != s0.kind) return fail(HPCGX_ESTATE, "ranks planned different steps");
+    if (s0.kind == STEP_LAUNCH) {
+      for (int r = 0; r < P; ++r) TRY(plans[r][i].launch());
+    } else if (s0.kind == STEP_HALO) {
+      for (int r = 0; r < P; ++r) {
+        const Step &st = plans[r][i];
+        const LevelDev &A = g->ranks[r]->L[st.level];
+        const int64_t plane = (int64_t)A.nx * A.ny;
+        const size_t pb = (size_t)plane * st.esize;
+        const char *v = static_cast<const char *>(st.vec);
+        if (r + 1 < P)   // last plane -> lower halo of the rank above
+          CK(cudaMemcpyAsync(static_cast<char *>(plans[r + 1][i].vec) - pb,
+                             v + (A.n - plane) * st.esize, pb, cudaMemcpyDeviceToDevice, s));
+        if (r > 0)       // first plane -> upper halo of the rank below
+          CK(cudaMemcpyAsync(static_cast<char *>(plans[r - 1][i].vec) + A.n * st.esize, v, pb,
+                             cudaMemcpyDeviceToDevice, s));
+      }
+    } else {
+      p0->note(launch_rank_sum(P, g->bufs, s0.nv, s));
+      if (s0.fin >= 0)
+        for (hpcgx_problem *pr : g->ranks)
+          pr->note(launch_finish(s0.fin, s0.nv, pr->gsum, pr->st, s));
+    }
+  }
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+Runner single_runner(hpcgx_problem *p) {
+  return [p](std::vector<Plan> &plans) { return run_plan(p, plans[0]); };
+}
+Runner group_runner(hpcgx_group *g) {
+  return [g](std::vector<Plan> &plans) { return group_run(g, plans); };
+}
+
+// CG over the ranks (src/CG.cpp:76-130 with the reductions of every rank
+// summed): the same iteration as the one-GPU solver, run step by step; the
+// host reads the stop flag (identical on every rank) once per iteration.
+int sharded_cg(const std::vector<hpcgx_problem *> &ps, const Runner &run, int kind,
+               const double *const *b, double *const *x, int max_iter, double tol, int *niters,
+               double *normr, double *normr0) {
+  if (max_iter < 0) return fail(HPCGX_EINVAL, "max_iter < 0");
+  const size_t P = ps.size();
+  CgState h;
+  std::memset(&h, 0, sizeof(h));
+  h.tol = tol;
+  h.max_iter = max_iter;
+  h.flexible = kind == G_MIXED;
+  std::vector<Plan> init(P), iter(P);
+  for (size_t r = 0; r < P; ++r) {
+    hpcgx_problem *p = ps[r];
+    TRY(p->check_ready(kind == G_MIXED));
+    if (!b[r] || !x[r]) return fail(HPCGX_EINVAL, "null vector");
+    CK(cudaMemcpyAsync(p->st, &h, sizeof(h), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(p->x, x[r], p->L[0].n * sizeof(double), cudaMemcpyDeviceToDevice,
+                       p->stream));
+    p->plan_cg_init(init[r], kind, b[r]);
+    p->plan_cg_iteration(iter[r], kind);
+  }
+  TRY(run(init));
+  hpcgx_problem *p0 = ps[0];
+  while (true) {
+    CK(cudaMemcpyAsync(&h, p0->st, sizeof(h), cudaMemcpyDeviceToHost, p0->stream));
+    CK(cudaStreamSynchronize(p0->stream));
+    if (h.done) break;
+    TRY(run(iter));
+  }
+  for (size_t r = 0; r < P; ++r)
+    CK(cudaMemcpyAsync(x[r], ps[r]->x, ps[r]->L[0].n * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ps[r]->stream));
+  for (hpcgx_problem *p : ps) CK(cudaStreamSynchronize(p->stream));
+  if (niters) *niters = h.niters;
+  if (normr) *normr = h.normr;
+  if (normr0) *normr0 = h.normr0;
+  if (h.nonfinite) return fail(HPCGX_ENONFINITE, "CG: residual norm is not finite");
+  return HPCGX_OK;
+}
+
+// A one-step operator (SpMV / SYMGS / V-cycle) over the ranks.
+template <class BUILD>
+int sharded_op(const std::vector<hpcgx_problem *> &ps, const Runner &run, BUILD build) {
+  std::vector<Plan> plans(ps.size());
+  for (size_t r = 0; r < ps.size(); ++r) TRY(build(ps[r], plans[r], (int)r));
+  TRY(run(plans));
+  for (hpcgx_problem *p : ps) {
+    CK(cudaStreamSynchronize(p->stream));
+  }
+  CK(cudaGetLastError());
+  return HPCGX_OK;
+}
+
+// The per-problem operators of a sharded problem run over its communicator.
+int need_comm(hpcgx_problem *p) {
+  if (p->nranks > 1 && !p->nccl)
+    return fail(HPCGX_ESTATE, "sharded problem: attach a communicator or use a group");
+  return HPCGX_OK;
+}
+
+int group_kind(int mode, int *kind) {
+  switch (mode) {
+    case HPCGX_CG_PLAIN: *kind = G_FP64_NOPREC; return HPCGX_OK;
+    case HPCGX_CG_MG: *kind = G_FP64_PREC; return HPCGX_OK;
+    case HPCGX_CG_MIXED: *kind = G_MIXED; return HPCGX_OK;
+    default: return fail(HPCGX_EINVAL, "unknown CG mode");
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 const char *hpcgx_last_error(void) { return g_err.c_str(); }
@@ -611,11 +1111,17 @@ const char *hpcgx_last_error(void) { return g_err.c_str(); }
 int hpcgx_version(void) { return 1; }
 
 int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem **out) {
+  return hpcgx_create_slab(device, nx, ny, nz, levels, 1, 0, out);
+}
+
+int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks, int rank,
+                      hpcgx_problem **out) {
   if (!out) return fail(HPCGX_EINVAL, "out is NULL");
   *out = nullptr;
   if (nx < 1 || ny < 1 || nz < 1 || levels < 1 || levels > kMaxLevels)
     return fail(HPCGX_EINVAL, "bad geometry or level count");
-  if ((int64_t)nx * ny * nz >= (int64_t)1 << 31)
+  if (nranks < 1 || rank < 0 || rank >= nranks) return fail(HPCGX_EINVAL, "bad rank or rank count");
+  if ((int64_t)nx * ny * (nz + 2) >= (int64_t)1 << 31)
     return fail(HPCGX_EINVAL, "more than 2^31 rows: column indices are int32");
   for (int l = 0; l + 1 < levels; ++l)
     if (((nx >> l) & 1) || ((ny >> l) & 1) || ((nz >> l) & 1))
@@ -625,6 +1131,8 @@ int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem *
   hpcgx_problem *p = new hpcgx_problem;
   p->device = device;
   p->nlev = levels;
+  p->nranks = nranks;
+  p->rank = rank;
   int rc = HPCGX_OK;
   auto bail = [&](int code) {
     delete p;
@@ -637,22 +1145,29 @@ int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem *
   for (int l = 0; l < levels; ++l) {
     LevelDev &A = p->L[l];
     plan_level(A, nx >> l, ny >> l, nz >> l);
+    A.zlo = rank > 0;
+    A.zhi = rank + 1 < nranks;
     const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
     if ((rc = p->alloc((void **)&A.vals, slots * sizeof(double)))) return bail(rc);
     if ((rc = p->alloc((void **)&A.cols, slots * sizeof(int32_t)))) return bail(rc);
+    const int64_t plane = (int64_t)A.nx * A.ny;
     if (l > 0) {
       if ((rc = p->alloc((void **)&A.r64, A.n * sizeof(double)))) return bail(rc);
-      if ((rc = p->alloc((void **)&A.x64, A.n * sizeof(double)))) return bail(rc);
+      if ((rc = p->alloc_halo((void **)&A.x64, A.n, sizeof(double), plane))) return bail(rc);
       if ((rc = p->alloc((void **)&A.r32, A.n * sizeof(float)))) return bail(rc);
-      if ((rc = p->alloc((void **)&A.x32, A.n * sizeof(float)))) return bail(rc);
+      if ((rc = p->alloc_halo((void **)&A.x32, A.n, sizeof(float), plane))) return bail(rc);
     }
     red_cap = std::max<int64_t>(red_cap, A.spmv_blocks);
   }
   const int64_t n = p->L[0].n;
   red_cap = 2 * std::max<int64_t>(red_cap, vector_blocks(n));
-  for (double **v : {&p->b, &p->x, &p->r, &p->z, &p->p, &p->Ap, &p->tmp})
+  const int64_t plane0 = (int64_t)p->L[0].nx * p->L[0].ny;
+  for (double **v : {&p->b, &p->x, &p->r, &p->Ap, &p->tmp})
     if ((rc = p->alloc((void **)v, n * sizeof(double)))) return bail(rc);
-  if ((rc = p->alloc((void **)&p->z32, n * sizeof(float)))) return bail(rc);
+  for (double **v : {&p->z, &p->p})
+    if ((rc = p->alloc_halo((void **)v, n, sizeof(double), plane0))) return bail(rc);
+  if ((rc = p->alloc_halo((void **)&p->z32, n, sizeof(float), plane0))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->gsum, 2 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->result, 4 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->st, sizeof(CgState)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->red.partials, red_cap * sizeof(double)))) return bail(rc);
@@ -679,6 +1194,7 @@ int64_t hpcgx_rows(hpcgx_problem *p, int level) {
 int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz, const int32_t *cols,
                      const double *vals) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "sharded problems are generated on the device");
   if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
   return load_level_impl(
       p, level, [&](int64_t i) { return (int)nnz[i]; },
@@ -691,6 +1207,7 @@ int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz, const int3
 int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz,
                           const int32_t *const *cols, const double *const *vals) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "sharded problems are generated on the device");
   if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
   return load_level_impl(
       p, level, [&](int64_t i) { return (int)(unsigned char)nnz[i]; },
@@ -721,6 +1238,7 @@ int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma) {
     if (kind == HPCGX_GEN_HPCG) {
       p->note(launch_generate_hpcg(p->L[l], p->stream));
     } else if (kind == HPCGX_GEN_VARCOEF) {
+      if (p->nranks > 1) return fail(HPCGX_EINVAL, "variable coefficients: one rank only");
       p->note(launch_generate_varcoef(p->L[l], l, p->L[0].nx, p->L[0].ny, seed, sigma, p->stream));
     } else {
       return fail(HPCGX_EINVAL, "unknown generator kind");
@@ -796,6 +1314,12 @@ int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
   HANDLE(p);
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  if (p->sharded()) {
+    TRY(need_comm(p));
+    return sharded_op({p}, single_runner(p), [&](hpcgx_problem *q, Plan &pl, int) {
+      return q->plan_spmv(pl, level, x, y);
+    });
+  }
   p->note(launch_spmv(p->L[level], x, y, nullptr, 0, nullptr, nullptr, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   CK(cudaGetLastError());
@@ -804,6 +1328,7 @@ int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
 
 int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
   p->note(launch_spmv(p->L[level], x, y, nullptr, 0, nullptr, nullptr, p->stream, true));
@@ -816,6 +1341,12 @@ int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
   HANDLE(p);
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  if (p->sharded()) {
+    TRY(need_comm(p));
+    return sharded_op({p}, single_runner(p), [&](hpcgx_problem *q, Plan &pl, int) {
+      return q->plan_symgs(pl, level, r, x);
+    });
+  }
   TRY((p->symgs<double, double>(level, r, x)));
   CK(cudaStreamSynchronize(p->stream));
   CK(cudaGetLastError());
@@ -825,6 +1356,12 @@ int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
 int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
   HANDLE(p);
   TRY(p->check_ready(false));
+  if (p->sharded()) {
+    TRY(need_comm(p));
+    return sharded_op({p}, single_runner(p), [&](hpcgx_problem *q, Plan &pl, int) {
+      return q->plan_mg(pl, r, x);
+    });
+  }
   TRY((p->vcycle<double, double>(r, x, nullptr)));
   CK(cudaStreamSynchronize(p->stream));
   CK(cudaGetLastError());
@@ -833,6 +1370,7 @@ int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
 
 int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
   TRY(p->check_ready(true));
   p->note(launch_spmv32(p->L[level], x, y, p->stream));
@@ -844,6 +1382,7 @@ int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y) {
 int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const float *r32,
                       float *x) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
   TRY(p->check_ready(true));
   if ((r64 == nullptr) == (r32 == nullptr)) return fail(HPCGX_EINVAL, "give exactly one of r64, r32");
@@ -858,6 +1397,7 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
 
 int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(p->check_ready(true));
   TRY((p->vcycle<float, double>(r, x, nullptr)));
   CK(cudaStreamSynchronize(p->stream));
@@ -918,6 +1458,11 @@ int hpcgx_residual(hpcgx_problem *p, int64_t n, const double *v1, const double *
 int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
              int precond, int *niters, double *normr, double *normr0, double *times) {
   HANDLE(p);
+  if (p->sharded()) {
+    TRY(need_comm(p));
+    return sharded_cg({p}, single_runner(p), precond ? G_FP64_PREC : G_FP64_NOPREC, &b, &x,
+                      max_iter, tolerance, niters, normr, normr0);
+  }
   return p->cg(precond ? G_FP64_PREC : G_FP64_NOPREC, b, x, max_iter, tolerance, niters, normr,
                normr0, times);
 }
@@ -925,6 +1470,11 @@ int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double 
 int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
                    int *niters, double *normr, double *normr0, double *times) {
   HANDLE(p);
+  if (p->sharded()) {
+    TRY(need_comm(p));
+    return sharded_cg({p}, single_runner(p), G_MIXED, &b, &x, max_iter, tolerance, niters, normr,
+                      normr0);
+  }
   return p->cg(G_MIXED, b, x, max_iter, tolerance, niters, normr, normr0, times);
 }
 
@@ -941,7 +1491,15 @@ int hpcgx_cg_host(hpcgx_problem *p, int mode, const double *b_host, double *x_ho
   }
   CK(cudaMemcpyAsync(p->b, b_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
   CK(cudaMemcpyAsync(p->x, x_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-  TRY(p->cg(kind, p->b, p->x, max_iter, tolerance, niters, normr, normr0, times));
+  if (p->sharded()) {
+    TRY(need_comm(p));
+    const double *bd = p->b;
+    double *xd = p->x;
+    TRY(sharded_cg({p}, single_runner(p), kind, &bd, &xd, max_iter, tolerance, niters, normr,
+                   normr0));
+  } else {
+    TRY(p->cg(kind, p->b, p->x, max_iter, tolerance, niters, normr, normr0, times));
+  }
   CK(cudaMemcpyAsync(x_host, p->x, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   return HPCGX_OK;
@@ -1000,6 +1558,7 @@ int hpcgx_waxpby_host(hpcgx_problem *p, int64_t n, double alpha, const double *x
 
 int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, double *grad) {
   HANDLE(p);
+  if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   p->note(launch_adjoint_grad(p->L[0], lambda, x, grad, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   CK(cudaGetLastError());
@@ -1009,7 +1568,9 @@ int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, 
 int hpcgx_fill_uniform(hpcgx_problem *p, int64_t n, uint64_t seed, double lo, double hi,
                        double *v) {
   HANDLE(p);
-  p->note(launch_fill_uniform(n, seed, lo, hi, v, p->stream));
+  // a finest-level vector of a z-slab holds entries rank*n .. of the global one
+  const uint64_t offset = n == p->L[0].n ? (uint64_t)p->rank * (uint64_t)n : 0;
+  p->note(launch_fill_uniform(n, seed, offset, lo, hi, v, p->stream));
   CK(cudaStreamSynchronize(p->stream));
   CK(cudaGetLastError());
   return HPCGX_OK;
@@ -1061,6 +1622,114 @@ int hpcgx_synchronize(hpcgx_problem *p) {
   HANDLE(p);
   CK(cudaStreamSynchronize(p->stream));
   return HPCGX_OK;
+}
+
+// ---- sharding
+int hpcgx_nccl_unique_id(void *id, int bytes) {
+  if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");
+  NcclApi *api = nccl_api();
+  if (!api) return fail(HPCGX_ECOMM, "NCCL (libnccl.so.2) could not be loaded");
+  ncclUniqueId u;
+  NCCLCK(api->GetUniqueId(&u));
+  std::memcpy(id, &u, sizeof(u));
+  return HPCGX_OK;
+}
+
+int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
+  HANDLE(p);
+  if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");
+  if (p->nccl) return fail(HPCGX_ESTATE, "a communicator is attached already");
+  NcclApi *api = nccl_api();
+  if (!api) return fail(HPCGX_ECOMM, "NCCL (libnccl.so.2) could not be loaded");
+  ncclUniqueId u;
+  std::memcpy(&u, id, sizeof(u));
+  CK(cudaSetDevice(p->device));
+  NcclLink *link = new NcclLink;
+  ncclResult_t r = api->CommInitRank(&link->comm, p->nranks, u, p->rank);
+  if (r != ncclSuccess) {
+    delete link;
+    return fail(HPCGX_ECOMM, std::string("ncclCommInitRank: ") + api->GetErrorString(r));
+  }
+  p->nccl = link;
+  return HPCGX_OK;
+}
+
+int hpcgx_group_create(hpcgx_problem *const *ranks, int nranks, hpcgx_group **out) {
+  if (!out || !ranks || nranks < 1) return fail(HPCGX_EINVAL, "bad group arguments");
+  *out = nullptr;
+  for (int r = 0; r < nranks; ++r) {
+    hpcgx_problem *p = ranks[r];
+    if (!p) return fail(HPCGX_EINVAL, "null rank");
+    if (p->nranks != nranks || p->rank != r)
+      return fail(HPCGX_EINVAL, "rank r of the group must be slab r of nranks");
+    if (p->device != ranks[0]->device || p->nlev != ranks[0]->nlev ||
+        p->L[0].nx != ranks[0]->L[0].nx || p->L[0].ny != ranks[0]->L[0].ny ||
+        p->L[0].nz != ranks[0]->L[0].nz)
+      return fail(HPCGX_EINVAL, "group ranks differ in device or geometry");
+    if (p->nccl) return fail(HPCGX_ESTATE, "rank has a communicator attached");
+  }
+  CK(cudaSetDevice(ranks[0]->device));
+  std::unique_ptr<hpcgx_group> g(new hpcgx_group);
+  g->ranks.assign(ranks, ranks + nranks);
+  CK(cudaMalloc(&g->bufs, nranks * sizeof(double *)));
+  std::vector<double *> h(nranks);
+  for (int r = 0; r < nranks; ++r) h[r] = ranks[r]->gsum;
+  CK(cudaMemcpy(g->bufs, h.data(), nranks * sizeof(double *), cudaMemcpyHostToDevice));
+  // one stream for every rank: the lockstep order is the stream order
+  for (int r = 0; r < nranks; ++r) {
+    CK(cudaStreamSynchronize(ranks[r]->stream));
+    g->saved.push_back(ranks[r]->stream);
+  }
+  for (int r = 0; r < nranks; ++r) ranks[r]->stream = ranks[0]->stream;
+  *out = g.release();
+  return HPCGX_OK;
+}
+
+int hpcgx_group_destroy(hpcgx_group *g) {
+  if (!g) return HPCGX_OK;
+  if (!g->ranks.empty()) cudaStreamSynchronize(g->ranks[0]->stream);
+  for (size_t r = 0; r < g->ranks.size(); ++r) g->ranks[r]->stream = g->saved[r];
+  delete g;
+  return HPCGX_OK;
+}
+
+int hpcgx_group_spmv(hpcgx_group *g, int level, const double *const *x, double *const *y) {
+  if (!g || !x || !y) return fail(HPCGX_EINVAL, "null argument");
+  for (hpcgx_problem *p : g->ranks) {
+    TRY(check_level(p, level));
+    if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  }
+  return sharded_op(g->ranks, group_runner(g), [&](hpcgx_problem *q, Plan &pl, int r) {
+    return q->plan_spmv(pl, level, x[r], y[r]);
+  });
+}
+
+int hpcgx_group_symgs(hpcgx_group *g, int level, const double *const *r, double *const *x) {
+  if (!g || !r || !x) return fail(HPCGX_EINVAL, "null argument");
+  for (hpcgx_problem *p : g->ranks) {
+    TRY(check_level(p, level));
+    if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
+  }
+  return sharded_op(g->ranks, group_runner(g), [&](hpcgx_problem *q, Plan &pl, int k) {
+    return q->plan_symgs(pl, level, r[k], x[k]);
+  });
+}
+
+int hpcgx_group_mg(hpcgx_group *g, const double *const *r, double *const *x) {
+  if (!g || !r || !x) return fail(HPCGX_EINVAL, "null argument");
+  for (hpcgx_problem *p : g->ranks) TRY(p->check_ready(false));
+  return sharded_op(g->ranks, group_runner(g), [&](hpcgx_problem *q, Plan &pl, int k) {
+    return q->plan_mg(pl, r[k], x[k]);
+  });
+}
+
+int hpcgx_group_cg(hpcgx_group *g, int mode, const double *const *b, double *const *x,
+                   int max_iter, double tolerance, int *niters, double *normr, double *normr0) {
+  if (!g || !b || !x) return fail(HPCGX_EINVAL, "null argument");
+  int kind = 0;
+  TRY(group_kind(mode, &kind));
+  return sharded_cg(g->ranks, group_runner(g), kind, b, x, max_iter, tolerance, niters, normr,
+                    normr0);
 }
 
 }  // extern "C"

@@ -34,16 +34,23 @@ def _ptr(t):
 
 
 class Problem:
-    """One nx*ny*nz HPCG problem with ``levels`` multigrid levels on a GPU."""
+    """One nx*ny*nz HPCG problem with ``levels`` multigrid levels on a GPU.
 
-    def __init__(self, nx, ny, nz, levels=4, device=0):
+    With ``nranks`` > 1 it is z-slab ``rank`` of an nx*ny*(nz*nranks) problem
+    (the reference's 1 x 1 x nranks process grid): attach a communicator with
+    :meth:`attach_nccl` (one process per GPU) or tie all slabs of one process
+    into a :class:`Group`.
+    """
+
+    def __init__(self, nx, ny, nz, levels=4, device=0, nranks=1, rank=0):
         if not torch.cuda.is_available():
             raise RuntimeError("hpcg_b200 needs a CUDA device")
         self.dims = (nx, ny, nz)
         self.levels = levels
+        self.nranks, self.rank = nranks, rank
         self.device = torch.device("cuda", device)
         h = C.c_void_p()
-        check(lib().hpcgx_create(device, nx, ny, nz, levels, C.byref(h)))
+        check(lib().hpcgx_create_slab(device, nx, ny, nz, levels, nranks, rank, C.byref(h)))
         self.h = h
         self.stream = torch.cuda.Stream(device=self.device)
         check(lib().hpcgx_set_stream(self.h, C.c_void_p(self.stream.cuda_stream)))
@@ -72,6 +79,12 @@ class Problem:
 
     def rows(self, level=0):
         return int(lib().hpcgx_rows(self.h, level))
+
+    def attach_nccl(self, unique_id: bytes):
+        """Joins the NCCL communicator of the problem's ranks (collective); the
+        operators and CG then exchange halos and sum reductions over NCCL."""
+        buf = C.create_string_buffer(bytes(unique_id), _lib.NCCL_ID_BYTES)
+        check(lib().hpcgx_attach_nccl(self.h, buf, _lib.NCCL_ID_BYTES))
 
     def level_dims(self, level=0):
         nx, ny, nz = self.dims
@@ -272,3 +285,73 @@ class Problem:
 
     def synchronize(self):
         check(lib().hpcgx_synchronize(self.h))
+
+
+def nccl_unique_id() -> bytes:
+    """A fresh NCCL unique id (rank 0 makes it; every rank attaches with it)."""
+    buf = C.create_string_buffer(_lib.NCCL_ID_BYTES)
+    check(lib().hpcgx_nccl_unique_id(buf, _lib.NCCL_ID_BYTES))
+    return buf.raw
+
+
+def _ptrs(ts):
+    return (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
+
+
+class Group:
+    """Every z-slab of a sharded problem in one process on one GPU.
+
+    The slabs run in lockstep on the stream of slab 0: halo planes are copied
+    between the slabs' vectors and reductions are summed in rank order, which
+    is the multi-rank algorithm (block-Jacobi smoothing across slabs, sums over
+    ranks) on a single device.  Vector arguments are lists with one tensor per
+    rank.
+    """
+
+    def __init__(self, ranks):
+        self.ranks = list(ranks)
+        handles = (C.c_void_p * len(self.ranks))(*[p.h.value for p in self.ranks])
+        g = C.c_void_p()
+        check(lib().hpcgx_group_create(handles, len(self.ranks), C.byref(g)))
+        self.g = g
+        self.stream = self.ranks[0].stream
+
+    def close(self):
+        if getattr(self, "g", None):
+            lib().hpcgx_group_destroy(self.g)
+            self.g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _pre(self):
+        self.stream.wait_stream(torch.cuda.current_stream(self.ranks[0].device))
+
+    def spmv(self, xs, level=0):
+        self._pre()
+        ys = [p.empty(level) for p in self.ranks]
+        check(lib().hpcgx_group_spmv(self.g, level, _ptrs(xs), _ptrs(ys)))
+        return ys
+
+    def symgs(self, rs, xs, level=0):
+        """One symmetric sweep per slab (block Jacobi across slabs), x in place."""
+        self._pre()
+        check(lib().hpcgx_group_symgs(self.g, level, _ptrs(rs), _ptrs(xs)))
+        return xs
+
+    def mg(self, rs):
+        self._pre()
+        xs = [p.empty(0) for p in self.ranks]
+        check(lib().hpcgx_group_mg(self.g, _ptrs(rs), _ptrs(xs)))
+        return xs
+
+    def cg(self, bs, xs, max_iter, tol, mode=_lib.CG_MG):
+        """CG over the slabs; xs updated in place; returns (iters, normr, normr0)."""
+        self._pre()
+        k, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
+        check(lib().hpcgx_group_cg(self.g, mode, _ptrs(bs), _ptrs(xs), max_iter, tol,
+                                   C.byref(k), C.byref(nr), C.byref(nr0)))
+        return k.value, nr.value, nr0.value

@@ -33,11 +33,13 @@ extern "C" {
 #define HPCGX_ENONFINITE 4 /* CG met a non-finite residual norm           */
 #define HPCGX_ELAYOUT 5    /* matrix is not a 27-point stencil matrix     */
 #define HPCGX_ENOMEM 6     /* device allocation failed                    */
+#define HPCGX_ECOMM 7      /* a halo exchange or reduction across ranks failed */
 
 #define HPCGX_GEN_HPCG 0    /* the reference problem: 26 / -1 stencil     */
 #define HPCGX_GEN_VARCOEF 1 /* variable-coefficient SPD stencil           */
 
 typedef struct hpcgx_problem hpcgx_problem;
+typedef struct hpcgx_group hpcgx_group;
 
 const char *hpcgx_last_error(void);
 int hpcgx_version(void);
@@ -217,6 +219,45 @@ int hpcgx_probe_read(hpcgx_problem *p, int kind, double *ms, int64_t *launches, 
 int64_t hpcgx_launch_count(hpcgx_problem *p);
 /* Waits for all work of the problem's stream. */
 int hpcgx_synchronize(hpcgx_problem *p);
+
+/* ---- sharding over ranks (z-slabs) --------------------------------------
+ * The reference's MPI decomposition with a process grid of 1 x 1 x nranks
+ * (src/GenerateGeometry.cpp:49-169): rank r owns the planes r*nz .. r*nz+nz-1
+ * of an nx x ny x (nz*nranks) grid; every level coarsens its own slab
+ * (src/GenerateCoarseProblem.cpp:52).  SpMV and Gauss-Seidel read one halo
+ * plane from each neighbouring rank, exchanged where the reference calls
+ * ExchangeHalo (src/ExchangeHalo.cpp:34-110: before each SpMV and each
+ * SYMGS, src/ComputeSPMV_ref.cpp:55, src/ComputeSYMGS_ref.cpp:56), so the
+ * smoother is block Jacobi across ranks as in the reference; every dot
+ * product of CG is summed over the ranks (src/ComputeDotProduct_ref.cpp:66-77).
+ * Sharded problems are generated on the device (hpcgx_generate, HPCGX_GEN_HPCG);
+ * hpcgx_fill_uniform of a finest-level vector fills the rank's part of the
+ * global vector. */
+
+/* Creates slab `rank` of `nranks` (nz = planes per rank).  hpcgx_create is
+ * hpcgx_create_slab(..., 1, 0, ...). */
+int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks, int rank,
+                      hpcgx_problem **out);
+/* One process per GPU: rank 0 makes an NCCL unique id (bytes >= 128), every
+ * rank receives it (e.g. through torch.distributed) and attaches.  After
+ * that hpcgx_spmv, hpcgx_symgs, hpcgx_mg, hpcgx_cg, hpcgx_cg_mixed and
+ * hpcgx_cg_host are collective: every rank calls them with its own vectors.
+ * NCCL is loaded at run time (libnccl.so.2); HPCGX_ECOMM if it cannot be. */
+int hpcgx_nccl_unique_id(void *id, int bytes);
+int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes);
+/* Every rank in one process on one GPU (ranks[r] = slab r of nranks): the
+ * ranks run step by step in lockstep on one stream, halo planes are device
+ * copies and sums are taken in rank order.  Vector arguments are arrays of
+ * one device pointer per rank.  While the group exists its ranks run on the
+ * stream of rank 0; hpcgx_group_destroy gives every rank its stream back. */
+int hpcgx_group_create(hpcgx_problem *const *ranks, int nranks, hpcgx_group **out);
+int hpcgx_group_destroy(hpcgx_group *g);
+int hpcgx_group_spmv(hpcgx_group *g, int level, const double *const *x, double *const *y);
+int hpcgx_group_symgs(hpcgx_group *g, int level, const double *const *r, double *const *x);
+int hpcgx_group_mg(hpcgx_group *g, const double *const *r, double *const *x);
+/* mode: HPCGX_CG_PLAIN / HPCGX_CG_MG / HPCGX_CG_MIXED as for hpcgx_cg_host. */
+int hpcgx_group_cg(hpcgx_group *g, int mode, const double *const *b, double *const *x,
+                   int max_iter, double tolerance, int *niters, double *normr, double *normr0);
 /* Makes the library launch on `stream` (a cudaStream_t of the problem's
  * device, not the legacy default stream, since solvers capture CUDA graphs);
  * NULL returns to the problem's own stream.  Lets a caller order library

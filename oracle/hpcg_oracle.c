@@ -162,6 +162,48 @@ void or_symgs(int64_t nrow, const uint8_t *nnz, const int32_t *cols, const doubl
     gs_row(order ? order[k] : k, nnz, cols, vals, diag, r, x);
 }
 
+/* The SYMGS of a z-slab decomposition (slab_rows rows per rank): every rank
+ * runs ComputeSYMGS_ref (src/ComputeSYMGS_ref.cpp:53-100) on its own rows
+ * after ExchangeHalo (:56), so a row reads its own slab's current values and
+ * every other slab's values as they were when the sweep began -- for the
+ * forward and the backward sweep alike (block Jacobi across ranks).  With
+ * slab_rows == 0 this is or_symgs. */
+void or_symgs_slab(int64_t nrow, const uint8_t *nnz, const int32_t *cols, const double *vals,
+                   const int32_t *diag, const int64_t *order, int64_t slab_rows, const double *r,
+                   double *x) {
+  if (slab_rows <= 0 || slab_rows >= nrow) {
+    or_symgs(nrow, nnz, cols, vals, diag, order, r, x);
+    return;
+  }
+  double *x0 = (double *)malloc(sizeof(double) * (size_t)nrow);
+  memcpy(x0, x, sizeof(double) * (size_t)nrow);
+  for (int pass = 0; pass < 2; pass++) {
+    for (int64_t k = 0; k < nrow; k++) {
+      const int64_t kk = pass == 0 ? k : nrow - 1 - k;
+      const int64_t i = order ? order[kk] : kk;
+      const int64_t si = i / slab_rows;
+      const int32_t *c = cols + i * OR_STENCIL;
+      const double *v = vals + i * OR_STENCIL;
+      const double d = v[diag[i]];
+      double sum = r[i];
+      for (int j = 0; j < nnz[i]; j++) sum -= v[j] * (c[j] / slab_rows == si ? x[c[j]] : x0[c[j]]);
+      sum += x[i] * d;
+      x[i] = sum / d;
+    }
+  }
+  free(x0);
+}
+
+/* A dot product of the z-slab decomposition: every rank sums its rows in
+ * order (ComputeDotProduct_ref, src/ComputeDotProduct_ref.cpp:53-64), then
+ * the rank totals are summed in rank order (the MPI_Allreduce of :66-77). */
+double or_dot_slab(int64_t n, const double *x, const double *y, int64_t slab_rows) {
+  if (slab_rows <= 0 || slab_rows >= n) return or_dot(n, x, y);
+  double s = 0.0;
+  for (int64_t b = 0; b < n; b += slab_rows) s += or_dot(slab_rows, x + b, y + b);
+  return s;
+}
+
 /* Restates ComputeRestriction_ref (src/ComputeRestriction_ref.cpp:51). */
 void or_restriction(int64_t nc, const int32_t *f2c, const double *rf, const double *Axf,
                     double *rc) {
@@ -217,15 +259,15 @@ int or_mg(const or_level *L, int nlev, const double *r, double *x) {
   const or_level *A = &L[0];
   memset(x, 0, sizeof(double) * (size_t)A->nrow);
   if (nlev > 1 && A->f2c) {
-    or_symgs(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, r, x);
+    or_symgs_slab(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, A->slab_rows, r, x);
     or_spmv(A->nrow, A->nnz, A->cols, A->vals, x, A->Axf);
     or_restriction(A->nc, A->f2c, r, A->Axf, A->rc);
     int ierr = or_mg(L + 1, nlev - 1, A->rc, A->xc);
     if (ierr) return ierr;
     or_prolongation(A->nc, A->f2c, A->xc, x);
-    or_symgs(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, r, x);
+    or_symgs_slab(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, A->slab_rows, r, x);
   } else {
-    or_symgs(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, r, x);
+    or_symgs_slab(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, A->slab_rows, r, x);
   }
   return 0;
 }
@@ -245,7 +287,7 @@ int or_cg(const or_level *L, int nlev, const double *b, double *x, int max_iter,
   memcpy(p, x, sizeof(double) * (size_t)n);
   or_spmv(n, A->nnz, A->cols, A->vals, p, Ap);
   or_waxpby(n, 1.0, b, -1.0, Ap, r);
-  *normr = sqrt(or_dot(n, r, r));
+  *normr = sqrt(or_dot_slab(n, r, r, A->slab_rows));
   *normr0 = *normr;
   for (int k = 1; k <= max_iter && *normr / *normr0 > tolerance; k++) {
     if (precond) {
@@ -256,19 +298,19 @@ int or_cg(const or_level *L, int nlev, const double *b, double *x, int max_iter,
     }
     if (k == 1) {
       memcpy(p, z, sizeof(double) * (size_t)n);
-      rtz = or_dot(n, r, z);
+      rtz = or_dot_slab(n, r, z, A->slab_rows);
     } else {
       oldrtz = rtz;
-      rtz = or_dot(n, r, z);
+      rtz = or_dot_slab(n, r, z, A->slab_rows);
       beta = rtz / oldrtz;
       or_waxpby(n, 1.0, z, beta, p, p);
     }
     or_spmv(n, A->nnz, A->cols, A->vals, p, Ap);
-    pAp = or_dot(n, p, Ap);
+    pAp = or_dot_slab(n, p, Ap, A->slab_rows);
     alpha = rtz / pAp;
     or_waxpby(n, 1.0, x, alpha, p, x);
     or_waxpby(n, 1.0, r, -alpha, Ap, r);
-    *normr = sqrt(or_dot(n, r, r));
+    *normr = sqrt(or_dot_slab(n, r, r, A->slab_rows));
     *niters = k;
   }
   return 0;
@@ -374,11 +416,40 @@ void or_symgs32(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
     gs_row32(order ? order[k] : k, nnz, cols, vals, diag, r64, r32, x);
 }
 
+/* or_symgs_slab in FP32 with BF16 values. */
+void or_symgs32_slab(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
+                     const uint16_t *vals, const int32_t *diag, const int64_t *order,
+                     int64_t slab_rows, const double *r64, const float *r32, float *x) {
+  if (slab_rows <= 0 || slab_rows >= nrow) {
+    or_symgs32(nrow, nnz, cols, vals, diag, order, r64, r32, x);
+    return;
+  }
+  float *x0 = (float *)malloc(sizeof(float) * (size_t)nrow);
+  memcpy(x0, x, sizeof(float) * (size_t)nrow);
+  for (int pass = 0; pass < 2; pass++) {
+    for (int64_t k = 0; k < nrow; k++) {
+      const int64_t kk = pass == 0 ? k : nrow - 1 - k;
+      const int64_t i = order ? order[kk] : kk;
+      const int64_t si = i / slab_rows;
+      const int32_t *c = cols + i * OR_STENCIL;
+      const uint16_t *v = vals + i * OR_STENCIL;
+      const float d = or_float_from_bf16(v[diag[i]]);
+      float sum = r64 ? (float)r64[i] : r32[i];
+      for (int j = 0; j < nnz[i]; j++)
+        sum -= or_float_from_bf16(v[j]) * (c[j] / slab_rows == si ? x[c[j]] : x0[c[j]]);
+      sum += x[i] * d;
+      x[i] = sum / d;
+    }
+  }
+  free(x0);
+}
+
 /* The mixed-precision V-cycle: ComputeMG_ref's flow in FP32. */
 int or_mg32(const or_level32 *L, int nlev, const double *r64, const float *r32, float *x) {
   const or_level32 *A = &L[0];
   memset(x, 0, sizeof(float) * (size_t)A->nrow);
-  or_symgs32(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, r64, r32, x);
+  or_symgs32_slab(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, A->slab_rows, r64, r32,
+                  x);
   if (nlev > 1 && A->f2c) {
     or_spmv32(A->nrow, A->nnz, A->cols, A->vals, x, A->Axf);
     for (int64_t i = 0; i < A->nc; i++) {
@@ -389,7 +460,8 @@ int or_mg32(const or_level32 *L, int nlev, const double *r64, const float *r32, 
     int ierr = or_mg32(L + 1, nlev - 1, NULL, A->rc, A->xc);
     if (ierr) return ierr;
     for (int64_t i = 0; i < A->nc; i++) x[A->f2c[i]] += A->xc[i];
-    or_symgs32(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, r64, r32, x);
+    or_symgs32_slab(A->nrow, A->nnz, A->cols, A->vals, A->diag, A->order, A->slab_rows, r64, r32,
+                    x);
   }
   return 0;
 }
@@ -413,26 +485,26 @@ int or_fcg(const or_level *L64, const or_level32 *L32, int nlev, const double *b
   memcpy(p, x, sizeof(double) * (size_t)n);
   or_spmv(n, A->nnz, A->cols, A->vals, p, Ap);
   or_waxpby(n, 1.0, b, -1.0, Ap, r);
-  *normr = sqrt(or_dot(n, r, r));
+  *normr = sqrt(or_dot_slab(n, r, r, A->slab_rows));
   *normr0 = *normr;
   for (int k = 1; k <= max_iter && *normr / *normr0 > tolerance; k++) {
     int ierr = or_mg32(L32, nlev, r, NULL, z32);
     if (ierr) return ierr;
     for (int64_t i = 0; i < n; i++) z[i] = (double)z32[i];
-    rtz = or_dot(n, r, z);
+    rtz = or_dot_slab(n, r, z, A->slab_rows);
     if (k == 1) {
       memcpy(p, z, sizeof(double) * (size_t)n);
     } else {
-      double zAp = or_dot(n, z, Ap);
+      double zAp = or_dot_slab(n, z, Ap, A->slab_rows);
       beta = -zAp / pAp;
       or_waxpby(n, 1.0, z, beta, p, p);
     }
     or_spmv(n, A->nnz, A->cols, A->vals, p, Ap);
-    pAp = or_dot(n, p, Ap);
+    pAp = or_dot_slab(n, p, Ap, A->slab_rows);
     alpha = rtz / pAp;
     or_waxpby(n, 1.0, x, alpha, p, x);
     or_waxpby(n, 1.0, r, -alpha, Ap, r);
-    *normr = sqrt(or_dot(n, r, r));
+    *normr = sqrt(or_dot_slab(n, r, r, A->slab_rows));
     *niters = k;
   }
   return 0;

@@ -39,6 +39,7 @@ typedef struct or_level {
   double *Axf;            /* work: nrow                             */
   double *rc;             /* work: nc                               */
   double *xc;             /* work: nc                               */
+  int64_t slab_rows;      /* z-slab decomposition: rows per rank (0: one rank) */
 } or_level;
 
 /* One level of the mixed-precision hierarchy: BF16 values, FP32 vectors. */
@@ -54,6 +55,7 @@ typedef struct or_level32 {
   float *Axf;
   float *rc;
   float *xc;
+  int64_t slab_rows;
 } or_level32;
 
 /* --- problem generation ------------------------------------------------ */
@@ -74,6 +76,11 @@ void or_restriction(int64_t nc, const int32_t *f2c, const double *rf, const doub
                     double *rc);
 void or_prolongation(int64_t nc, const int32_t *f2c, const double *xc, double *xf);
 double or_dot(int64_t n, const double *x, const double *y);
+/* z-slab decomposition (slab_rows rows per rank, 0: one rank) */
+void or_symgs_slab(int64_t nrow, const uint8_t *nnz, const int32_t *cols, const double *vals,
+                   const int32_t *diag, const int64_t *order, int64_t slab_rows, const double *r,
+                   double *x);
+double or_dot_slab(int64_t n, const double *x, const double *y, int64_t slab_rows);
 void or_waxpby(int64_t n, double alpha, const double *x, double beta, const double *y,
                double *w);
 double or_residual(int64_t n, const double *v1, const double *v2);
@@ -95,6 +102,9 @@ void or_spmv32(int64_t nrow, const uint8_t *nnz, const int32_t *cols, const uint
 void or_symgs32(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
                 const uint16_t *vals, const int32_t *diag, const int64_t *order,
                 const double *r64, const float *r32, float *x);
+void or_symgs32_slab(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
+                     const uint16_t *vals, const int32_t *diag, const int64_t *order,
+                     int64_t slab_rows, const double *r64, const float *r32, float *x);
 int or_mg32(const or_level32 *L, int nlev, const double *r64, const float *r32, float *x);
 int or_fcg(const or_level *L64, const or_level32 *L32, int nlev, const double *b,
            double *x, int max_iter, double tolerance, int *niters, double *normr,

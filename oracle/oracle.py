@@ -36,13 +36,17 @@ def build(quiet: bool = True) -> None:
 
 
 def _ptr(a):
-    return None if a is None else a.ctypes.data_as(_P)
+    if a is None:
+        return None
+    if not a.flags.c_contiguous:
+        raise ValueError("oracle arrays must be C-contiguous")
+    return a.ctypes.data_as(_P)
 
 
 class _Level(C.Structure):
     _fields_ = [("nrow", _I64), ("nnz", _P), ("cols", _P), ("vals", _P), ("diag", _P),
                 ("order", _P), ("f2c", _P), ("nc", _I64), ("Axf", _P), ("rc", _P),
-                ("xc", _P)]
+                ("xc", _P), ("slab_rows", _I64)]
 
 
 class Level:
@@ -54,6 +58,7 @@ class Level:
         self.nnz, self.cols, self.vals, self.diag, self.f2c = nnz, cols, vals, diag, f2c
         self.order = None        # SYMGS visiting order (int64) or None
         self.position = None     # natural row -> position in colour order
+        self.slab_rows = 0       # z-slab decomposition: rows per rank (0: one rank)
 
     @property
     def vals_bf16(self):
@@ -95,6 +100,8 @@ class Oracle:
                                                 _D, _P, _P, _P, _P]
             lib.or_waxpby.argtypes = [_I64, _D, _P, _D, _P, _P]
             lib.or_dot.argtypes = [_I64, _P, _P]
+            lib.or_dot_slab.restype = _D
+            lib.or_dot_slab.argtypes = [_I64, _P, _P, _I64]
             lib.or_residual.argtypes = [_I64, _P, _P]
             lib.or_bf16_from_double.restype = C.c_uint16
             lib.or_bf16_from_double.argtypes = [_D]
@@ -160,6 +167,19 @@ class Oracle:
         return L, b, x, xe
 
     @classmethod
+    def slab_hierarchy(cls, nx, ny, nz, nranks, levels=LEVELS):
+        """The hierarchy of a z-slab decomposition into nranks slabs of nz planes
+        (a 1 x 1 x nranks process grid, src/GenerateGeometry.cpp:49-169): the
+        global grid nx x ny x (nz nranks) and its injection, every slab
+        coarsening its own planes (src/GenerateCoarseProblem.cpp:52), with
+        .slab_rows set on every level for the block-Jacobi smoother and the
+        per-rank dot products."""
+        L, b, x, xe = cls.hierarchy(nx, ny, nz * nranks, levels)
+        for l, lev in enumerate(L):
+            lev.slab_rows = (nx >> l) * (ny >> l) * (nz >> l) if nranks > 1 else 0
+        return L, b, x, xe
+
+    @classmethod
     def colour_order(cls, L):
         """Greedy colouring (src/OptimizeProblem.cpp:43-96) on every level;
         sets .position (natural -> colour order) and .order (its inverse)."""
@@ -194,8 +214,9 @@ class Oracle:
     def symgs(cls, lev, r, x, coloured=False):
         x = x.copy()
         order = lev.order if coloured else None
-        cls.lib().or_symgs(_I64(lev.nrow), _ptr(lev.nnz), _ptr(lev.cols), _ptr(lev.vals),
-                           _ptr(lev.diag), _ptr(order), _ptr(r), _ptr(x))
+        cls.lib().or_symgs_slab(_I64(lev.nrow), _ptr(lev.nnz), _ptr(lev.cols), _ptr(lev.vals),
+                                _ptr(lev.diag), _ptr(order), _I64(lev.slab_rows), _ptr(r),
+                                _ptr(x))
         return x
 
     @classmethod
@@ -221,8 +242,8 @@ class Oracle:
         return xf
 
     @classmethod
-    def dot(cls, x, y):
-        return cls.lib().or_dot(x.size, _ptr(x), _ptr(y))
+    def dot(cls, x, y, slab_rows=0):
+        return cls.lib().or_dot_slab(x.size, _ptr(x), _ptr(y), slab_rows)
 
     @classmethod
     def waxpby(cls, alpha, x, beta, y):
@@ -244,7 +265,7 @@ class Oracle:
             keep += [Axf, rc, xc]
             arr[i] = _Level(lev.nrow, _ptr(lev.nnz), _ptr(lev.cols), _ptr(lev.vals), _ptr(lev.diag),
                             _ptr(lev.order) if coloured else None, _ptr(lev.f2c), nc, _ptr(Axf),
-                            _ptr(rc), _ptr(xc))
+                            _ptr(rc), _ptr(xc), lev.slab_rows)
         return arr, keep
 
     @staticmethod
@@ -258,7 +279,7 @@ class Oracle:
             keep += [Axf, rc, xc]
             arr[i] = _Level(lev.nrow, _ptr(lev.nnz), _ptr(lev.cols), _ptr(lev.vals_bf16),
                             _ptr(lev.diag), _ptr(lev.order) if coloured else None, _ptr(lev.f2c),
-                            nc, _ptr(Axf), _ptr(rc), _ptr(xc))
+                            nc, _ptr(Axf), _ptr(rc), _ptr(xc), lev.slab_rows)
         return arr, keep
 
     @classmethod
