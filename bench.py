@@ -11,15 +11,21 @@ it for the mixed-vs-FP64 comparison.  Inputs are generated on the device
   value        seconds per mixed solve (mean of --steps timed solves), lower is better
   e2e          the same through the C ABI from pinned host buffers (b and x0
                copied in, x copied out inside the timed region)
-  roofline     finest-level Gauss-Seidel class kernel (the dominant kernel):
-               algorithmic bytes / CUDA-event duration of every launch in the
-               timed region, against the measured HBM copy bandwidth
+  roofline     the largest kernel, the mixed solver's FP64 SpMV (and, beside
+               it, the finest-level Gauss-Seidel class kernels): algorithmic
+               bytes / CUDA-event duration of every launch in the timed region,
+               against the measured HBM copy bandwidth
   cpu_baseline the reference's own CG_ref (oracle/_ref, OpenMP on all host
                cores) per-iteration time on a 128^3 sample, scaled to 512^3
                rows and to the FP64 solve's iteration count
 
-Multi-GPU (torchrun): every rank solves its own 512^3 system (the path is
-replicated, not sharded, in this build); value is the max over ranks.
+Multi-GPU (torchrun, N ranks): one system of N z-slabs, each GPU holding one
+512^3 slab (weak scaling; the reference's 1 x 1 x N process grid): halo planes
+are exchanged and dot products summed over NCCL, the smoother is block Jacobi
+across slabs as in the reference, so the iteration count depends on N.  value
+is the max over ranks of the solve time.  --replicas runs N independent
+systems instead.  The sharded solver runs step by step without CUDA graphs,
+so the per-kernel probes (roofline) are reported at N = 1 only.
 """
 from __future__ import annotations
 
@@ -130,6 +136,16 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def sum_over_ranks(values, dist=None, device=None):
+    """Element-wise sum of a list of floats over all ranks (identity on one rank)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return list(values)
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return t.tolist()
+
+
 def max_over_ranks(values, dist=None, device=None):
     """Element-wise max of a list of floats over all ranks (identity on one rank).
     Every rank must call it with the same number of values."""
@@ -197,12 +213,18 @@ def run_reference(args, dims):
     print(json.dumps(out))
 
 
-def config(dims):
-    return {"workload": "HPCG %dx%dx%d (b = A u, u~U(-1,1) seed 1, x0 = 0): mixed-precision "
-                        "flexible PCG (FP32/BF16 V-cycle, FP64 outer) to FP64 rel. residual "
-                        "1e-10, compared with plain FP64 PCG" % dims,
-            "grid": list(dims), "levels": 4, "smoother": "8-colour symmetric Gauss-Seidel",
-            "tolerance": TOL, "l2": "no flush: every step streams > 60 GB, far above the 126 MB L2"}
+def config(dims, world=1, sharded=False):
+    g = (dims[0], dims[1], dims[2] * world) if sharded else dims
+    c = {"workload": "HPCG %dx%dx%d (b = A u, u~U(-1,1) seed 1, x0 = 0): mixed-precision "
+                     "flexible PCG (FP32/BF16 V-cycle, FP64 outer) to FP64 rel. residual "
+                     "1e-10, compared with plain FP64 PCG" % g,
+         "grid": list(g), "levels": 4, "smoother": "8-colour symmetric Gauss-Seidel",
+         "tolerance": TOL, "l2": "no flush: every step streams > 60 GB, far above the 126 MB L2"}
+    if world > 1:
+        c["parallelism"] = ("z-slabs over %d GPUs (%dx%dx%d per GPU), NCCL halo exchange and "
+                            "sums" % ((world,) + tuple(dims)) if sharded else
+                            "%d independent replicas" % world)
+    return c
 
 
 def run_varcoef(args):
@@ -289,6 +311,11 @@ def main():
     ap.add_argument("--grid", type=int, nargs="+", default=[512])
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with --gpus N: N independent systems instead of one system sharded "
+                         "into N z-slabs")
+    ap.add_argument("--sharded", action="store_true",
+                    help="the sharded step-by-step solver with an NCCL communicator even on one GPU")
     ap.add_argument("--clocks-csv", default="",
                     help="keep the nvidia-smi clock samples here (%%d = rank)")
     ap.add_argument("--ref-iters", type=int, default=0,
@@ -313,6 +340,10 @@ def main():
         return
 
     import torch
+    # NCCL writes its log (a version line when NCCL_DEBUG is set) to stdout by
+    # default; this process prints exactly one JSON line there
+    os.environ.setdefault("NCCL_DEBUG_FILE",
+                          os.path.join(tempfile.gettempdir(), "hpcgx_bench_nccl.%h.%p.log"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -325,7 +356,7 @@ def main():
     dev = local
     torch.cuda.set_device(dev)
 
-    from hpcg_b200 import Problem
+    from hpcg_b200 import Problem, nccl_unique_id
     from hpcg_b200._lib import PROBE_GS_FINE, PROBE_GS_FINE_BWD, PROBE_SPMV_FINE
 
     def barrier():
@@ -334,9 +365,25 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    P = Problem(*dims, device=dev)
+    # N > 1: one nx x ny x (nz N) system, z-slab `rank` on this GPU (weak
+    # scaling: every GPU holds one dims-sized slab), halos and sums over NCCL
+    sharded = (world > 1 and not args.replicas) or args.sharded
+    if sharded:
+        P = Problem(*dims, device=dev, nranks=world, rank=rank)
+    else:
+        P = Problem(*dims, device=dev)
     P.generate("hpcg")
     P.build_mixed()
+    if sharded:
+        uid = [nccl_unique_id() if rank == 0 else None]
+        if dist:
+            dist.broadcast_object_list(uid, src=0, device=torch.device("cuda", dev))
+        P.attach_nccl(uid[0])
+
+    def gnorm(v):
+        """2-norm of the global vector whose slab this rank holds."""
+        s = float(torch.dot(v, v))
+        return sum_over_ranks([s], dist if (sharded and dist) else None, f"cuda:{dev}")[0] ** 0.5
     n = P.rows()
     u = P.fill_uniform(SEED_U, -1.0, 1.0)
     b = P.spmv(u)
@@ -383,7 +430,7 @@ def main():
     t_mixed = statistics.mean(times)
     relres_mixed = nr / nr0
     x_mixed = x.clone()
-    true_mixed = (torch.linalg.norm(b - P.spmv(x_mixed)) / torch.linalg.norm(b)).item()
+    true_mixed = gnorm(b - P.spmv(x_mixed)) / gnorm(b)
 
     # ---------------- FP64 comparison
     solve(False)
@@ -399,9 +446,9 @@ def main():
         t64.append(e0.elapsed_time(e1) * 1e-3)
     t_fp64 = statistics.mean(t64)
     x64 = x.clone()
-    true_fp64 = (torch.linalg.norm(b - P.spmv(x64)) / torch.linalg.norm(b)).item()
-    x_diff = (torch.linalg.norm(x_mixed - x64) / torch.linalg.norm(x64)).item()
-    err_u = (torch.linalg.norm(x_mixed - u) / torch.linalg.norm(u)).item()
+    true_fp64 = gnorm(b - P.spmv(x64)) / gnorm(b)
+    x_diff = gnorm(x_mixed - x64) / gnorm(x64)
+    err_u = gnorm(x_mixed - u) / gnorm(u)
 
     # ---------------- end to end through the C ABI from pinned host buffers
     bh = b.cpu().pin_memory()
@@ -417,10 +464,11 @@ def main():
 
     flops, b64, b32, n0, z0 = model(dims)
     peak, peak_kind = peaks()
-    gf_mixed = flops * iters_mixed[-1] / t_mixed / 1e9
-    gf_fp64 = flops * k64 / t_fp64 / 1e9
-    hbm_mixed = b32 * iters_mixed[-1] / t_mixed / 1e9
-    hbm_fp64 = b64 * k64 / t_fp64 / 1e9
+    # whole job: every rank does one slab's (or one replica's) work per iteration
+    gf_mixed = world * flops * iters_mixed[-1] / t_mixed / 1e9
+    gf_fp64 = world * flops * k64 / t_fp64 / 1e9
+    hbm_mixed = world * b32 * iters_mixed[-1] / t_mixed / 1e9
+    hbm_fp64 = world * b64 * k64 / t_fp64 / 1e9
     traffic = {}
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic_%d.json" % dims[0])
     if os.path.exists(tpath) and dims[0] == dims[1] == dims[2]:
@@ -455,7 +503,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": t_mixed * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp64 outer / fp32+bf16 V-cycle",
         "data": "synthetic (HPCG-generated problem on the device, b = A u)",
-        "config": config(dims),
+        "config": config(dims, world, sharded),
         "iterations": {"mixed": iters_mixed[-1], "fp64": k64},
         "fp64_time_s": t_fp64,
         "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
@@ -471,8 +519,8 @@ def main():
         "roofline": roofline(PROBE_SPMV_FINE, "k_spmv<double,double,1,1>"),
         "roofline_gs_bwd": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f64>"),
         "roofline_gs_fine_all_modes": roofline(PROBE_GS_FINE, "k_gs_class finest level, all modes"),
-        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": 2 * n * 8,
-                "d2h_bytes_per_step": n * 8},
+        "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": world * 2 * n * 8,
+                "d2h_bytes_per_step": world * n * 8},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": cpu,

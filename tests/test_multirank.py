@@ -1,6 +1,6 @@
 """Host logic of bench.py's multi-GPU mode on CPU ranks (gloo, world size 2):
-every rank runs its own problem replica and the reported time is the max over
-ranks.  No GPU is needed."""
+the reported time is the max over ranks and global norms sum the ranks'
+squares.  No GPU is needed."""
 import os
 import socket
 
@@ -29,8 +29,9 @@ def _worker(rank, world, port, out):
     import bench
     vals = [1.0 + rank, 10.0 - rank, 0.5 * rank]
     got = bench.max_over_ranks(vals, dist)
+    tot = bench.sum_over_ranks(vals, dist)
     dist.barrier()
-    out[rank] = got
+    out[rank] = (got, tot)
     dist.destroy_process_group()
 
 
@@ -39,9 +40,10 @@ def test_max_over_ranks_two_gloo_ranks():
     mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_worker, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
-    assert out[0] == out[1] == [2.0, 10.0, 0.5]
+    assert out[0] == out[1] == ([2.0, 10.0, 0.5], [3.0, 19.0, 0.5])
 
 
 def test_max_over_ranks_single_process():
     import bench
     assert bench.max_over_ranks([3.0, 4.0]) == [3.0, 4.0]
+    assert bench.sum_over_ranks([3.0, 4.0]) == [3.0, 4.0]
