@@ -227,6 +227,65 @@ def config(dims, world=1, sharded=False):
     return c
 
 
+def run_kernels(args):
+    """Each plain operator of the reference's API on its own (256^3 by default):
+    CUDA-event time of every call on the library's stream, algorithmic bytes of
+    the reference implementation's step (real nonzeros only: SpMV 12 nnz + 16 n,
+    SYMGS 24 nnz + 48 n, dot 16 n, WAXPBY 24 n) and their ratio against the
+    measured HBM copy bandwidth.  Before each timed call the stream writes a
+    256 MB buffer (L2 is 126 MB), so every call starts cold, and the stream is
+    busy while the host enqueues the call; the calls are blocking API calls, so
+    the time of the short vector operators still includes the launch of the
+    call and the copy of its result to the host.  The command for the
+    per-kernel ncu DRAM captures."""
+    import torch
+    from hpcg_b200 import Problem
+    g = args.grid
+    dims = (g[0], g[0], g[0]) if len(g) == 1 else tuple(g)
+    torch.cuda.set_device(0)
+    P = Problem(*dims)
+    P.generate("hpcg")
+    P.build_mixed()
+    n = P.rows()
+    flops, b64, b32, n0, nnz = model(dims)
+    u = P.fill_uniform(SEED_U, -1.0, 1.0)
+    v = P.fill_uniform(SEED_U + 1, 0.0, 1.0)
+    x = P.fill_uniform(SEED_U + 2, 0.0, 1.0)
+    y = torch.empty_like(u)
+    u32 = u.float()
+    ops = {
+        "spmv": (lambda: P.spmv(u, y=y), 12 * nnz + 16 * n),
+        "spmv_stencil": (lambda: P.spmv(u, y=y, stencil_cols=True), 8 * nnz + 16 * n),
+        "symgs": (lambda: P.symgs(v, x), 24 * nnz + 48 * n),
+        "dot": (lambda: P.dot(u, v), 16 * n),
+        "waxpby": (lambda: P.waxpby(0.7, u, -1.3, v, w=y), 24 * n),
+        "spmv_bf16": (lambda: P.spmv_mixed(u32), 2 * nnz + 8 * n),
+    }
+    peak, peak_kind = peaks()
+    out = {"workload": "kernels", "grid": list(dims), "unit": "GB/s", "peak_gbs": peak,
+           "peak_kind": peak_kind, "steps": args.steps, "warmup": args.warmup, "ops": {}}
+    s = P.stream
+    flush = torch.empty(32 << 20, dtype=torch.float64, device="cuda")
+    for name, (f, nbytes) in ops.items():
+        for _ in range(args.warmup):
+            f()
+        ts = []
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                flush.fill_(0.0)
+            e0.record(s)
+            f()
+            e1.record(s)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) * 1e-3)
+        t = statistics.mean(ts)
+        out["ops"][name] = {"ms": t * 1e3, "algorithmic_bytes": nbytes,
+                            "achieved_gbs": nbytes / t / 1e9, "frac": nbytes / t / 1e9 / peak}
+    print(json.dumps(out))
+    P.close()
+
+
 def run_varcoef(args):
     """Differentiable-solve workloads (no reference counterpart):
     (3) 128^3, a_ij = -exp(0.5 z) (seed 2), b ~ U(0,1), x_target ~ N(0,1) (seed 3),
@@ -322,13 +381,17 @@ def main():
                     help="iterations the reference arm scales to (0: measured FP64 count)")
     ap.add_argument("--ref-sample", type=int, default=128)
     ap.add_argument("--ref-sample-it", type=int, default=10)
-    ap.add_argument("--workload", default="pcg", choices=["pcg", "varcoef"],
-                    help="pcg: the headline metric; varcoef: the differentiable-solve checks")
+    ap.add_argument("--workload", default="pcg", choices=["pcg", "varcoef", "kernels"],
+                    help="pcg: the headline metric; varcoef: the differentiable-solve checks; "
+                         "kernels: each plain operator on its own (give --grid 256)")
     ap.add_argument("--grid3", type=int, default=128)
     ap.add_argument("--grid4", type=int, nargs=3, default=[512, 512, 256])
     args = ap.parse_args()
     if args.workload == "varcoef":
         run_varcoef(args)
+        return
+    if args.workload == "kernels":
+        run_kernels(args)
         return
     g = args.grid
     dims = (g[0], g[0], g[0]) if len(g) == 1 else tuple(g)
