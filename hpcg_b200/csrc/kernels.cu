@@ -52,42 +52,20 @@ __device__ __forceinline__ double warp_red(double v) {
   return MAX ? warp_max(v) : warp_sum(v);
 }
 
-// Reduces NV values over the block and publishes one partial per block; the
-// last block to arrive sums all partials in block order and returns true with
-// the totals in tot (valid in every thread of that block).  Deterministic for
-// a fixed grid size.
-template <int NV, bool MAX = false>
-__device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&tot)[NV]) {
-  __shared__ double sh[NV][32];
-  __shared__ double fin[NV];
-  __shared__ int amlast;
+// Sums (or maxes) `count` partials p[0], p[stride], ... over the block in a
+// fixed order (strided per thread, warp tree, warps in order); the result is
+// valid in every thread.
+template <int NV, bool MAX>
+__device__ void block_sum_partials(const double *p, int64_t count, int64_t stride,
+                                   double (&out)[NV], double (&sh)[NV][32]) {
+  __shared__ double res[NV];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int i = 0; i < NV; ++i) {
-    double t = warp_red<MAX>(v[i]);
-    if (lane == 0) sh[i][wid] = t;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-      double t = MAX ? 0.0 : 0.0;
-      for (int w = 0; w < nw; ++w) t = MAX ? fmax(t, sh[i][w]) : t + sh[i][w];
-      red.partials[(int64_t)i * gridDim.x + blockIdx.x] = t;
-    }
-    __threadfence();
-    unsigned int prev = atomicAdd(red.counter, 1u);
-    amlast = (prev == gridDim.x - 1);
-  }
-  __syncthreads();
-  if (!amlast) return false;
-  __threadfence();
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
     double t = 0.0;
-    for (int64_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-      double p = __ldcg(red.partials + (int64_t)i * gridDim.x + b);
-      t = MAX ? fmax(t, p) : t + p;
+    for (int64_t b = threadIdx.x; b < count; b += blockDim.x) {
+      const double q = __ldcg(p + (int64_t)i * stride + b);
+      t = MAX ? fmax(t, q) : t + q;
     }
     t = warp_red<MAX>(t);
     __syncthreads();
@@ -96,12 +74,77 @@ __device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&tot)[NV
     if (threadIdx.x == 0) {
       double s = 0.0;
       for (int w = 0; w < nw; ++w) s = MAX ? fmax(s, sh[i][w]) : s + sh[i][w];
-      fin[i] = s;
+      res[i] = s;
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < NV; ++i) tot[i] = fin[i];
+  for (int i = 0; i < NV; ++i) out[i] = res[i];
+}
+
+// Reduces NV values over the block and publishes one partial per block; the
+// last block to arrive returns true with the totals in tot (valid in every
+// thread of that block).  Up to kReduceGroup blocks the last block sums the
+// partials in block order.  Larger grids (the SpMV's one block per line
+// group) reduce in two levels so that no counter takes more than
+// kReduceGroup atomics and no block reads more than that many partials: the
+// last block of each group of kReduceGroup sums its group's partials in block
+// order, and the last group sums the group totals in group order.
+// Deterministic for a fixed grid size either way.
+constexpr int kReduceGroup = 1024;
+template <int NV, bool MAX = false>
+__device__ bool grid_reduce(double (&v)[NV], const Reduce &red, double (&tot)[NV]) {
+  __shared__ double sh[NV][32];
+  __shared__ int amlast;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  const int64_t G = gridDim.x;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double t = warp_red<MAX>(v[i]);
+    if (lane == 0) sh[i][wid] = t;
+  }
+  __syncthreads();
+  const int64_t ngroups = (G + kReduceGroup - 1) / kReduceGroup;
+  const int64_t group = blockIdx.x / kReduceGroup;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t = MAX ? fmax(t, sh[i][w]) : t + sh[i][w];
+      red.partials[(int64_t)i * G + blockIdx.x] = t;
+    }
+    __threadfence();
+    const int64_t gsize = ngroups == 1 ? G : min((int64_t)kReduceGroup, G - group * kReduceGroup);
+    unsigned int *ctr = ngroups == 1 ? red.counter : red.counter + 1 + group;
+    const unsigned int prev = atomicAdd(ctr, 1u);
+    amlast = (prev == gsize - 1);
+  }
+  __syncthreads();
+  if (!amlast) return false;
+  __threadfence();
+  if (ngroups == 1) {
+    block_sum_partials<NV, MAX>(red.partials, G, G, tot, sh);
+    if (threadIdx.x == 0) *red.counter = 0u;
+    return true;
+  }
+  // last block of its group: the group's total, then the group-level count
+  const int64_t base = group * kReduceGroup;
+  const int64_t gsize = min((int64_t)kReduceGroup, G - base);
+  double gt[NV];
+  block_sum_partials<NV, MAX>(red.partials + base, gsize, G, gt, sh);
+  double *gp = red.partials + (int64_t)NV * G;   // group totals
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) gp[(int64_t)i * ngroups + group] = gt[i];
+    red.counter[1 + group] = 0u;
+    __threadfence();
+    const unsigned int prev = atomicAdd(red.counter, 1u);
+    amlast = (prev == ngroups - 1);
+  }
+  __syncthreads();
+  if (!amlast) return false;
+  __threadfence();
+  block_sum_partials<NV, MAX>(gp, ngroups, ngroups, tot, sh);
   if (threadIdx.x == 0) *red.counter = 0u;
   return true;
 }

@@ -41,8 +41,8 @@ struct CgState {
 // Scratch of the deterministic grid reductions: per-block partial sums and a
 // completion counter (reset to zero by the last block).
 struct Reduce {
-  double *partials = nullptr;
-  unsigned int *counter = nullptr;
+  double *partials = nullptr;   // NV per block, then NV per group of 1024 blocks
+  unsigned int *counter = nullptr;   // [0]: blocks or groups done; [1 + g]: group g
   int64_t capacity = 0;       // doubles in partials
   // Sharded solve: the last block stores this rank's totals here instead of
   // applying the scalar step, which launch_finish applies after the totals

@@ -1171,9 +1171,10 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   if ((rc = p->alloc((void **)&p->result, 4 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->st, sizeof(CgState)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->red.partials, red_cap * sizeof(double)))) return bail(rc);
-  if ((rc = p->alloc((void **)&p->red.counter, sizeof(unsigned int)))) return bail(rc);
+  const int64_t ncounters = 1 + (red_cap + 1023) / 1024;   // top counter + one per group
+  if ((rc = p->alloc((void **)&p->red.counter, ncounters * sizeof(unsigned int)))) return bail(rc);
   p->red.capacity = red_cap;
-  e = cudaMemsetAsync(p->red.counter, 0, sizeof(unsigned int), p->stream);
+  e = cudaMemsetAsync(p->red.counter, 0, ncounters * sizeof(unsigned int), p->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
   if (e != cudaSuccess) return bail(fail(HPCGX_ECUDA, cudaGetErrorString(e)));
   *out = p;
