@@ -12,7 +12,7 @@ struct LevelDev {
   int64_t cstart[8] = {}, ccount[8] = {};
   ClassInfo cls[4] = {};
   int lines_per_block[4] = {}, blocks[4] = {}, threads[4] = {};
-  int spmv_blocks = 0;        // all four classes in one launch
+  int spmv_blocks = 0;        // all four classes in one launch (one line group per block)
   // z-slab of a sharded problem: a neighbouring rank owns the plane below
   // (zlo) / above (zhi); vectors read by SpMV and Gauss-Seidel then hold one
   // halo plane on each side (indices -nx*ny..-1 and n..n+nx*ny-1)
