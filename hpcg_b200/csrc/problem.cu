@@ -378,8 +378,8 @@ struct hpcgx_problem {
     }
     for (int i = 0; i < 5; ++i)
       if (!phase[kind][i]) CK(cudaEventCreate(&phase[kind][i]));
-    // every launch a probe can bracket in one iteration: 16 class launches
-    // per level and sweep pair, plus the SpMV
+    // every launch a probe can bracket in one iteration: 14 class launches
+    // per level (two symmetric sweeps of 7), plus the SpMV, with room to spare
     const size_t need = 16 * kMaxLevels + 1;
     if (probe != HPCGX_PROBE_NONE) {
       // events of earlier graphs may still be referenced: keep them, add new
