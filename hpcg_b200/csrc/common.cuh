@@ -129,6 +129,20 @@ __device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, 
 __device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float rn_div(float a, float b) { return __fdiv_rn(a, b); }
 
+// Accumulation steps s + a b and s - a b.  FP64 rounds the product and the
+// sum separately, as the reference's x86-64 build does (it emits no FMA), so
+// the FP64 path stays bit-exact with it; the FP32 arithmetic of the mixed
+// V-cycle (no reference counterpart) uses one fused multiply-add, as its
+// oracle does with C's fmaf.
+__device__ __forceinline__ double mac_add(double s, double a, double b) {
+  return __dadd_rn(s, __dmul_rn(a, b));
+}
+__device__ __forceinline__ double mac_sub(double s, double a, double b) {
+  return __dsub_rn(s, __dmul_rn(a, b));
+}
+__device__ __forceinline__ float mac_add(float s, float a, float b) { return __fmaf_rn(a, b, s); }
+__device__ __forceinline__ float mac_sub(float s, float a, float b) { return __fmaf_rn(-a, b, s); }
+
 // Matrix value -> arithmetic type.
 __device__ __forceinline__ double to_arith(double v, double) { return v; }
 __device__ __forceinline__ float to_arith(uint16_t h, float) {

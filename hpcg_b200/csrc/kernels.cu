@@ -460,7 +460,7 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
       for (int s = 0; s < HPCGX_STENCIL; ++s) xv[s] = __ldg(x + col[s]);
       T sum = T(0);
 #pragma unroll
-      for (int s = 0; s < HPCGX_STENCIL; ++s) sum = rn_add(sum, rn_mul(to_arith(val[s], T()), xv[s]));
+      for (int s = 0; s < HPCGX_STENCIL; ++s) sum = mac_add(sum, to_arith(val[s], T()), xv[s]);
       const T xrow = xv[HPCGX_DIAG_SLOT];
       y[id.row] = sum;
       if (DOT) acc += (double)xrow * (double)sum;
@@ -533,26 +533,26 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
 #pragma unroll
   for (int s = 0; s < HPCGX_STENCIL; ++s) {
     if (s == HPCGX_DIAG_SLOT) {
-      if (!ZERO) sum = rn_sub(sum, rn_mul(d, xi));
+      if (!ZERO) sum = mac_sub(sum, d, xi);
       continue;
     }
     if (ZERO && (((c ^ slot_mask(s)) > c) || val[s] == T(0))) continue;
-    sum = rn_sub(sum, rn_mul(val[s], xv[s]));
+    sum = mac_sub(sum, val[s], xv[s]);
   }
-  if (!ZERO) sum = rn_add(sum, rn_mul(xi, d));
+  if (!ZERO) sum = mac_add(sum, xi, d);
   const T xn = rn_div(sum, d);
   if (SYM) {
     T sum2 = rhs;
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s) {
       if (s == HPCGX_DIAG_SLOT) {
-        sum2 = rn_sub(sum2, rn_mul(d, xn));
+        sum2 = mac_sub(sum2, d, xn);
         continue;
       }
       if (val[s] == T(0)) continue;   // a product with 0: no change
-      sum2 = rn_sub(sum2, rn_mul(val[s], xv[s]));
+      sum2 = mac_sub(sum2, val[s], xv[s]);
     }
-    sum2 = rn_add(sum2, rn_mul(xn, d));
+    sum2 = mac_add(sum2, xn, d);
     x[id.row] = rn_div(sum2, d);
     return;
   }
@@ -561,7 +561,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
     T ax = T(0);
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s)
-      ax = rn_add(ax, rn_mul(val[s], s == HPCGX_DIAG_SLOT ? xn : xv[s]));
+      ax = mac_add(ax, val[s], s == HPCGX_DIAG_SLOT ? xn : xv[s]);
     rc[crow] = rn_sub(rhs, ax);
   }
 }
@@ -668,7 +668,7 @@ k_restrict_residual(LevelMat<VT> A, ClassInfo C0, int64_t nc, const RT *__restri
     if (IMPLICIT) stencil_cols<true>(A, id, NeedAll(), col);
     T ax = T(0);
 #pragma unroll
-    for (int s = 0; s < HPCGX_STENCIL; ++s) ax = rn_add(ax, rn_mul(val[s], x[col[s]]));
+    for (int s = 0; s < HPCGX_STENCIL; ++s) ax = mac_add(ax, val[s], x[col[s]]);
     rc[i] = rn_sub(vec_to(__ldg(rf + id.row), T()), ax);
   }
 }

@@ -382,13 +382,16 @@ void or_vals_to_bf16(int64_t n, const double *v, uint16_t *h) {
   for (int64_t i = 0; i < n; i++) h[i] = or_bf16_from_double(v[i]);
 }
 
+/* The mixed V-cycle's FP32 arithmetic accumulates with fused multiply-adds
+ * (C's fmaf, correctly rounded): sum + v x and sum - v x in one rounding each,
+ * in the row's entry order. */
 void or_spmv32(int64_t nrow, const uint8_t *nnz, const int32_t *cols, const uint16_t *vals,
                const float *x, float *y) {
   for (int64_t i = 0; i < nrow; i++) {
     float sum = 0.0f;
     const int32_t *c = cols + i * OR_STENCIL;
     const uint16_t *v = vals + i * OR_STENCIL;
-    for (int j = 0; j < nnz[i]; j++) sum += or_float_from_bf16(v[j]) * x[c[j]];
+    for (int j = 0; j < nnz[i]; j++) sum = fmaf(or_float_from_bf16(v[j]), x[c[j]], sum);
     y[i] = sum;
   }
 }
@@ -400,8 +403,8 @@ static inline void gs_row32(int64_t i, const uint8_t *nnz, const int32_t *cols,
   const uint16_t *v = vals + i * OR_STENCIL;
   const float d = or_float_from_bf16(v[diag[i]]);
   float sum = r64 ? (float)r64[i] : r32[i];
-  for (int j = 0; j < nnz[i]; j++) sum -= or_float_from_bf16(v[j]) * x[c[j]];
-  sum += x[i] * d;
+  for (int j = 0; j < nnz[i]; j++) sum = fmaf(-or_float_from_bf16(v[j]), x[c[j]], sum);
+  sum = fmaf(x[i], d, sum);
   x[i] = sum / d;
 }
 
@@ -436,8 +439,8 @@ void or_symgs32_slab(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
       const float d = or_float_from_bf16(v[diag[i]]);
       float sum = r64 ? (float)r64[i] : r32[i];
       for (int j = 0; j < nnz[i]; j++)
-        sum -= or_float_from_bf16(v[j]) * (c[j] / slab_rows == si ? x[c[j]] : x0[c[j]]);
-      sum += x[i] * d;
+        sum = fmaf(-or_float_from_bf16(v[j]), c[j] / slab_rows == si ? x[c[j]] : x0[c[j]], sum);
+      sum = fmaf(x[i], d, sum);
       x[i] = sum / d;
     }
   }
