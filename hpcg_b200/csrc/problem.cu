@@ -1108,7 +1108,7 @@ extern "C" {
 
 const char *hpcgx_last_error(void) { return g_err.c_str(); }
 
-int hpcgx_version(void) { return 1; }
+int hpcgx_version(void) { return 2; }   // 2: sharding (slabs, NCCL, groups)
 
 int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem **out) {
   return hpcgx_create_slab(device, nx, ny, nz, levels, 1, 0, out);

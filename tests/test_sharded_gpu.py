@@ -158,6 +158,21 @@ def test_one_rank_sharded_paths_reproduce_fused_solver(oracle):
     ref.close()
 
 
+def test_group_checks_its_ranks(oracle):
+    from hpcg_b200 import Group, HPCGXError, Problem
+    a = Problem(16, 16, 8, nranks=2, rank=0)
+    b = Problem(16, 16, 8, nranks=2, rank=1)
+    c = Problem(16, 8, 8, nranks=2, rank=1)
+    with pytest.raises(HPCGXError):
+        Group([b, a])                  # rank r must sit at position r
+    with pytest.raises(HPCGXError):
+        Group([a, c])                  # slabs of different geometry
+    with pytest.raises(HPCGXError):
+        Group([a])                     # slab 0 of 2 alone
+    for p in (a, b, c):
+        p.close()
+
+
 def test_sharded_problem_needs_a_backend(oracle):
     from hpcg_b200 import HPCGXError, Problem
     p = Problem(16, 16, 8, nranks=2, rank=1)
