@@ -21,6 +21,11 @@ _IP = C.POINTER(C.c_int)
 _DP = C.POINTER(C.c_double)
 _I64P = C.POINTER(C.c_int64)
 
+# hpcgx_halo_fn / hpcgx_sum_fn (include/hpcgx.h)
+HALO_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                      C.c_int64, C.c_int, C.c_void_p)
+SUM_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
+
 # name -> (restype, argtypes); mirrors include/hpcgx.h
 SIGNATURES = {
     "hpcgx_last_error": (C.c_char_p, []),
@@ -70,6 +75,7 @@ SIGNATURES = {
     "hpcgx_create_slab": (_I, [_I, _I, _I, _I, _I, _I, _I, C.POINTER(_P)]),
     "hpcgx_nccl_unique_id": (_I, [_P, _I]),
     "hpcgx_attach_nccl": (_I, [_P, _P, _I]),
+    "hpcgx_attach_comm": (_I, [_P, HALO_FN, SUM_FN, _P]),
     "hpcgx_group_create": (_I, [_P, _I, C.POINTER(_P)]),
     "hpcgx_group_destroy": (_I, [_P]),
     "hpcgx_group_spmv": (_I, [_P, _I, _P, _P]),

@@ -140,9 +140,12 @@ struct hpcgx_problem {
   // is nx x ny x (nz nranks) (src/GenerateGeometry.cpp with npx = npy = 1)
   int nranks = 1, rank = 0;
   struct NcclLink *nccl = nullptr;   // exchange backend, one process per GPU
+  hpcgx_halo_fn comm_halo = nullptr; // caller-provided exchange backend
+  hpcgx_sum_fn comm_sum = nullptr;
+  void *comm_ctx = nullptr;
   double *gsum = nullptr;            // this rank's deferred reduction totals
   double *hstage[kMaxLevels] = {};   // haloed FP64 staging of operator inputs
-  bool sharded() const { return nranks > 1 || nccl != nullptr; }
+  bool sharded() const { return nranks > 1 || nccl != nullptr || comm_halo != nullptr; }
 
   ~hpcgx_problem();
   int alloc(void **ptr, size_t n) {
@@ -946,18 +949,39 @@ int nccl_halo(hpcgx_problem *p, int l, void *v, int esize) {
   return HPCGX_OK;
 }
 
-// Runs one rank's plan: halo steps over NCCL, sums as an all-reduce of the
-// deferred totals.  Without a communicator (one rank) both are no-ops.
+// The same exchange through the caller's halo function.
+int callback_halo(hpcgx_problem *p, int l, void *v, int esize) {
+  const LevelDev &A = p->L[l];
+  if (!A.zlo && !A.zhi) return HPCGX_OK;
+  const int64_t plane = (int64_t)A.nx * A.ny;
+  char *b = static_cast<char *>(v);
+  void *send_lo = A.zlo ? b : nullptr;
+  void *recv_lo = A.zlo ? b - plane * esize : nullptr;
+  void *send_hi = A.zhi ? b + (A.n - plane) * esize : nullptr;
+  void *recv_hi = A.zhi ? b + A.n * esize : nullptr;
+  if (p->comm_halo(p->comm_ctx, send_lo, recv_lo, send_hi, recv_hi, plane, esize,
+                   static_cast<void *>(p->stream)) != 0)
+    return fail(HPCGX_ECOMM, "the halo function failed");
+  return HPCGX_OK;
+}
+
+// Runs one rank's plan: halo steps and sums of the deferred totals over the
+// attached backend (NCCL or the caller's functions).  Without one (one rank)
+// both are no-ops.
 int run_plan(hpcgx_problem *p, Plan &pl) {
   for (Step &s : pl) {
     if (s.kind == STEP_LAUNCH) {
       TRY(s.launch());
     } else if (s.kind == STEP_HALO) {
       if (p->nccl) TRY(nccl_halo(p, s.level, s.vec, s.esize));
+      else if (p->comm_halo) TRY(callback_halo(p, s.level, s.vec, s.esize));
     } else {
       if (p->nccl)
         NCCLCK(nccl_api()->AllReduce(p->gsum, p->gsum, s.nv, ncclFloat64, ncclSum, p->nccl->comm,
                                      p->stream));
+      else if (p->comm_sum &&
+               p->comm_sum(p->comm_ctx, p->gsum, s.nv, static_cast<void *>(p->stream)) != 0)
+        return fail(HPCGX_ECOMM, "the sum function failed");
       if (s.fin >= 0) p->note(launch_finish(s.fin, s.nv, p->gsum, p->st, p->stream));
     }
   }
@@ -1088,7 +1112,7 @@ int sharded_op(const std::vector<hpcgx_problem *> &ps, const Runner &run, BUILD 
 
 // The per-problem operators of a sharded problem run over its communicator.
 int need_comm(hpcgx_problem *p) {
-  if (p->nranks > 1 && !p->nccl)
+  if (p->nranks > 1 && !p->nccl && !p->comm_halo)
     return fail(HPCGX_ESTATE, "sharded problem: attach a communicator or use a group");
   return HPCGX_OK;
 }
@@ -1639,7 +1663,7 @@ int hpcgx_nccl_unique_id(void *id, int bytes) {
 int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
   HANDLE(p);
   if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");
-  if (p->nccl) return fail(HPCGX_ESTATE, "a communicator is attached already");
+  if (p->nccl || p->comm_halo) return fail(HPCGX_ESTATE, "a communicator is attached already");
   NcclApi *api = nccl_api();
   if (!api) return fail(HPCGX_ECOMM, "NCCL (libnccl.so.2) could not be loaded");
   ncclUniqueId u;
@@ -1655,6 +1679,16 @@ int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
   return HPCGX_OK;
 }
 
+int hpcgx_attach_comm(hpcgx_problem *p, hpcgx_halo_fn halo, hpcgx_sum_fn sum, void *ctx) {
+  HANDLE(p);
+  if (!halo || !sum) return fail(HPCGX_EINVAL, "both functions are needed");
+  if (p->nccl || p->comm_halo) return fail(HPCGX_ESTATE, "a communicator is attached already");
+  p->comm_halo = halo;
+  p->comm_sum = sum;
+  p->comm_ctx = ctx;
+  return HPCGX_OK;
+}
+
 int hpcgx_group_create(hpcgx_problem *const *ranks, int nranks, hpcgx_group **out) {
   if (!out || !ranks || nranks < 1) return fail(HPCGX_EINVAL, "bad group arguments");
   *out = nullptr;
@@ -1667,7 +1701,7 @@ int hpcgx_group_create(hpcgx_problem *const *ranks, int nranks, hpcgx_group **ou
         p->L[0].nx != ranks[0]->L[0].nx || p->L[0].ny != ranks[0]->L[0].ny ||
         p->L[0].nz != ranks[0]->L[0].nz)
       return fail(HPCGX_EINVAL, "group ranks differ in device or geometry");
-    if (p->nccl) return fail(HPCGX_ESTATE, "rank has a communicator attached");
+    if (p->nccl || p->comm_halo) return fail(HPCGX_ESTATE, "rank has a communicator attached");
   }
   CK(cudaSetDevice(ranks[0]->device));
   std::unique_ptr<hpcgx_group> g(new hpcgx_group);

@@ -86,6 +86,70 @@ class Problem:
         buf = C.create_string_buffer(bytes(unique_id), _lib.NCCL_ID_BYTES)
         check(lib().hpcgx_attach_nccl(self.h, buf, _lib.NCCL_ID_BYTES))
 
+    def attach_comm(self, halo, sum_):
+        """A caller's own transport (hpcgx_attach_comm): ``halo(send_lo, recv_lo,
+        send_hi, recv_hi, count, esize, stream)`` and ``sum_(buf, count, stream)``
+        take device pointers (int, 0 = no neighbour) and the library's stream
+        handle, and return nothing; an exception becomes HPCGX_ECOMM."""
+        import traceback
+
+        def _halo(ctx, slo, rlo, shi, rhi, count, esize, stream):
+            try:
+                halo(slo or 0, rlo or 0, shi or 0, rhi or 0, int(count), int(esize), stream or 0)
+                return 0
+            except Exception:
+                traceback.print_exc()
+                return 1
+
+        def _sum(ctx, buf, count, stream):
+            try:
+                sum_(buf or 0, int(count), stream or 0)
+                return 0
+            except Exception:
+                traceback.print_exc()
+                return 1
+
+        self._comm_fns = (_lib.HALO_FN(_halo), _lib.SUM_FN(_sum))   # kept alive with the problem
+        check(lib().hpcgx_attach_comm(self.h, self._comm_fns[0], self._comm_fns[1], None))
+
+    def attach_torch_distributed(self, group=None):
+        """Exchanges halos and sums over torch.distributed (any backend; gloo
+        moves them through host memory), rank = this problem's slab."""
+        import torch.distributed as dist
+        dev = self.device
+
+        def view(ptr, count, esize):
+            typestr = "<f8" if esize == 8 else "<f4"
+            return torch.as_tensor(_DeviceArray(ptr, count, typestr), device=dev)
+
+        def on_host(t):
+            return t.cpu() if dist.get_backend(group) == "gloo" else t
+
+        def halo(slo, rlo, shi, rhi, count, esize, stream):
+            torch.cuda.ExternalStream(stream, device=dev).synchronize()
+            reqs, into = [], []
+            for send, recv, peer in ((slo, rlo, self.rank - 1), (shi, rhi, self.rank + 1)):
+                if not send:
+                    continue
+                out = on_host(view(send, count, esize).clone())
+                got = torch.empty_like(out)
+                reqs += [dist.isend(out, peer, group=group), dist.irecv(got, peer, group=group)]
+                into.append((recv, got))
+            for q in reqs:
+                q.wait()
+            for recv, got in into:
+                view(recv, count, esize).copy_(got)
+            torch.cuda.synchronize(dev)
+
+        def sum_(buf, count, stream):
+            torch.cuda.ExternalStream(stream, device=dev).synchronize()
+            t = on_host(view(buf, count, 8).clone())
+            dist.all_reduce(t, group=group)
+            view(buf, count, 8).copy_(t)
+            torch.cuda.synchronize(dev)
+
+        self.attach_comm(halo, sum_)
+
     def level_dims(self, level=0):
         nx, ny, nz = self.dims
         return nx >> level, ny >> level, nz >> level
@@ -292,6 +356,15 @@ def nccl_unique_id() -> bytes:
     buf = C.create_string_buffer(_lib.NCCL_ID_BYTES)
     check(lib().hpcgx_nccl_unique_id(buf, _lib.NCCL_ID_BYTES))
     return buf.raw
+
+
+class _DeviceArray:
+    """A device buffer owned by the library, seen by torch through the CUDA
+    array interface."""
+
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3, "strides": None}
 
 
 def _ptrs(ts):

@@ -245,6 +245,22 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
  * NCCL is loaded at run time (libnccl.so.2); HPCGX_ECOMM if it cannot be. */
 int hpcgx_nccl_unique_id(void *id, int bytes);
 int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes);
+/* A caller's own transport (MPI, a host channel, ...) instead of NCCL:
+ *   halo(ctx, send_lo, recv_lo, send_hi, recv_hi, count, esize, stream)
+ *     sends `count` elements of esize bytes at send_lo to the rank below and
+ *     receives as many from it into recv_lo, and the same with the rank above
+ *     through send_hi / recv_hi (both NULL where there is no such rank); the
+ *     pointers are device memory, valid once the work queued on `stream` (a
+ *     cudaStream_t) has run;
+ *   sum(ctx, buf, count, stream) replaces the `count` device doubles at buf
+ *     by their sum over the ranks, every rank receiving the same values.
+ * Both return 0 on success; the library turns anything else into
+ * HPCGX_ECOMM.  After the call the operators and CG are collective, as with
+ * hpcgx_attach_nccl. */
+typedef int (*hpcgx_halo_fn)(void *ctx, void *send_lo, void *recv_lo, void *send_hi,
+                             void *recv_hi, int64_t count, int esize, void *stream);
+typedef int (*hpcgx_sum_fn)(void *ctx, double *buf, int count, void *stream);
+int hpcgx_attach_comm(hpcgx_problem *p, hpcgx_halo_fn halo, hpcgx_sum_fn sum, void *ctx);
 /* Every rank in one process on one GPU (ranks[r] = slab r of nranks): the
  * ranks run step by step in lockstep on one stream, halo planes are device
  * copies and sums are taken in rank order.  Vector arguments are arrays of
