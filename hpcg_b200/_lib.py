@@ -86,7 +86,7 @@ SIGNATURES = {
 
 HPCGX_OK = 0
 ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ESTATE", 4: "ENONFINITE", 5: "ELAYOUT", 6: "ENOMEM",
-          7: "ECOMM"}
+          7: "ECOMM", 8: "ETIMEOUT"}
 NCCL_ID_BYTES = 128
 GEN_HPCG, GEN_VARCOEF = 0, 1
 PROBE_NONE, PROBE_GS_FINE, PROBE_SPMV_FINE, PROBE_GS_FINE_BWD = 0, 1, 2, 4

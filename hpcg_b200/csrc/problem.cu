@@ -9,12 +9,14 @@
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nccl.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <memory>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -37,12 +39,24 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+// The status of a failed CUDA call, its error taken off the thread's
+// last-error slot as CK does.
+int cuda_fail(cudaError_t e) {
+  cudaGetLastError();
+  return fail(e == cudaErrorMemoryAllocation ? HPCGX_ENOMEM : HPCGX_ECUDA, cudaGetErrorString(e));
+}
+
+// A failed CUDA call becomes the returned status; its error is also taken
+// off the thread's last-error slot, so that a later call does not report it
+// a second time (errors that break the context persist regardless).
 #define CK(call)                                                                  \
   do {                                                                            \
     cudaError_t e_ = (call);                                                      \
-    if (e_ != cudaSuccess)                                                        \
+    if (e_ != cudaSuccess) {                                                      \
+      cudaGetLastError();                                                         \
       return fail(e_ == cudaErrorMemoryAllocation ? HPCGX_ENOMEM : HPCGX_ECUDA,   \
                   std::string(#call) + ": " + cudaGetErrorString(e_));            \
+    }                                                                             \
   } while (0)
 
 #define TRY(expr)               \
@@ -50,6 +64,13 @@ int fail(int code, const std::string &msg) {
     int rc_ = (expr);           \
     if (rc_ != HPCGX_OK) return rc_; \
   } while (0)
+
+// A named range around each library call for timeline tools (NVTX; costs a
+// pointer test when no tool is attached).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
@@ -152,6 +173,7 @@ struct hpcgx_problem {
     cudaError_t e = cudaMalloc(ptr, n);
     if (e != cudaSuccess) {
       *ptr = nullptr;
+      cudaGetLastError();   // reported through the status; do not leave it for a later call
       return fail(HPCGX_ENOMEM, "cudaMalloc of " + std::to_string(n) + " bytes failed: " +
                                     cudaGetErrorString(e));
     }
@@ -747,7 +769,7 @@ namespace {
   do {                                                                     \
     if (!(p)) return fail(HPCGX_EINVAL, "null problem handle");            \
     cudaError_t e_ = cudaSetDevice((p)->device);                          \
-    if (e_ != cudaSuccess) return fail(HPCGX_ECUDA, cudaGetErrorString(e_)); \
+    if (e_ != cudaSuccess) return cuda_fail(e_);                        \
   } while (0)
 
 int check_level(hpcgx_problem *p, int level) {
@@ -1054,6 +1076,44 @@ Runner group_runner(hpcgx_group *g) {
   return [g](std::vector<Plan> &plans) { return group_run(g, plans); };
 }
 
+// Waits for the work queued on s, for at most HPCGX_WAIT_TIMEOUT_S seconds
+// (environment, default 600): on a sharded problem a rank whose peer has
+// failed then returns HPCGX_ETIMEOUT instead of blocking for ever behind an
+// exchange.  The queued work itself is left to finish.
+int bounded_wait(cudaStream_t s) {
+  static const double limit = [] {
+    const char *e = std::getenv("HPCGX_WAIT_TIMEOUT_S");
+    const double v = e ? std::atof(e) : 0.0;
+    return v > 0.0 ? v : 600.0;
+  }();
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, s);
+  const double t0 = now_s();
+  for (int polls = 0; e == cudaSuccess; ++polls) {
+    const cudaError_t q = cudaEventQuery(ev);
+    if (q != cudaErrorNotReady) {   // finished, or a real error
+      e = q;
+      break;
+    }
+    if (now_s() - t0 > limit) {
+      cudaEventDestroy(ev);
+      cudaGetLastError();           // the not-ready status of the last query
+      return fail(HPCGX_ETIMEOUT, "sharded work did not finish within HPCGX_WAIT_TIMEOUT_S = " +
+                                      std::to_string(limit) + " s");
+    }
+    if (polls > 2000) std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  cudaEventDestroy(ev);
+  if (e != cudaSuccess) return cuda_fail(e);
+  // a query that found the work unfinished leaves cudaErrorNotReady as the
+  // thread's last error, which is a status, not a failure: clear it
+  const cudaError_t last = cudaGetLastError();
+  if (last != cudaSuccess && last != cudaErrorNotReady)
+    return cuda_fail(last);
+  return HPCGX_OK;
+}
+
 // CG over the ranks (src/CG.cpp:76-130 with the reductions of every rank
 // summed): the same iteration as the one-GPU solver, run step by step; the
 // host reads the stop flag (identical on every rank) once per iteration.
@@ -1081,15 +1141,18 @@ int sharded_cg(const std::vector<hpcgx_problem *> &ps, const Runner &run, int ki
   TRY(run(init));
   hpcgx_problem *p0 = ps[0];
   while (true) {
+    // wait (bounded) first: a copy to pageable host memory would block
+    // without limit until the stream drains
+    TRY(bounded_wait(p0->stream));
     CK(cudaMemcpyAsync(&h, p0->st, sizeof(h), cudaMemcpyDeviceToHost, p0->stream));
-    CK(cudaStreamSynchronize(p0->stream));
+    CK(cudaStreamSynchronize(p0->stream));   // idle stream: returns at once
     if (h.done) break;
     TRY(run(iter));
   }
   for (size_t r = 0; r < P; ++r)
     CK(cudaMemcpyAsync(x[r], ps[r]->x, ps[r]->L[0].n * sizeof(double), cudaMemcpyDeviceToDevice,
                        ps[r]->stream));
-  for (hpcgx_problem *p : ps) CK(cudaStreamSynchronize(p->stream));
+  for (hpcgx_problem *p : ps) TRY(bounded_wait(p->stream));
   if (niters) *niters = h.niters;
   if (normr) *normr = h.normr;
   if (normr0) *normr0 = h.normr0;
@@ -1103,9 +1166,7 @@ int sharded_op(const std::vector<hpcgx_problem *> &ps, const Runner &run, BUILD 
   std::vector<Plan> plans(ps.size());
   for (size_t r = 0; r < ps.size(); ++r) TRY(build(ps[r], plans[r], (int)r));
   TRY(run(plans));
-  for (hpcgx_problem *p : ps) {
-    CK(cudaStreamSynchronize(p->stream));
-  }
+  for (hpcgx_problem *p : ps) TRY(bounded_wait(p->stream));
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1140,6 +1201,7 @@ int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem *
 
 int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks, int rank,
                       hpcgx_problem **out) {
+  NvtxRange range_("hpcgx_create_slab");
   if (!out) return fail(HPCGX_EINVAL, "out is NULL");
   *out = nullptr;
   if (nx < 1 || ny < 1 || nz < 1 || levels < 1 || levels > kMaxLevels)
@@ -1151,7 +1213,7 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
     if (((nx >> l) & 1) || ((ny >> l) & 1) || ((nz >> l) & 1))
       return fail(HPCGX_EINVAL, "level dimensions must be even to coarsen");
   cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) return fail(HPCGX_ECUDA, cudaGetErrorString(e));
+  if (e != cudaSuccess) return cuda_fail(e);
   hpcgx_problem *p = new hpcgx_problem;
   p->device = device;
   p->nlev = levels;
@@ -1163,7 +1225,7 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
     return code;
   };
   e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) return bail(fail(HPCGX_ECUDA, cudaGetErrorString(e)));
+  if (e != cudaSuccess) return bail(cuda_fail(e));
   p->stream = p->own_stream;
   int64_t red_cap = 0;
   for (int l = 0; l < levels; ++l) {
@@ -1200,7 +1262,7 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   p->red.capacity = red_cap;
   e = cudaMemsetAsync(p->red.counter, 0, ncounters * sizeof(unsigned int), p->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
-  if (e != cudaSuccess) return bail(fail(HPCGX_ECUDA, cudaGetErrorString(e)));
+  if (e != cudaSuccess) return bail(cuda_fail(e));
   *out = p;
   return HPCGX_OK;
 }
@@ -1218,6 +1280,7 @@ int64_t hpcgx_rows(hpcgx_problem *p, int level) {
 
 int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz, const int32_t *cols,
                      const double *vals) {
+  NvtxRange range_("hpcgx_load_level");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "sharded problems are generated on the device");
   if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
@@ -1231,6 +1294,7 @@ int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz, const int3
 
 int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz,
                           const int32_t *const *cols, const double *const *vals) {
+  NvtxRange range_("hpcgx_load_level_rows");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "sharded problems are generated on the device");
   if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
@@ -1258,6 +1322,7 @@ int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c, int64_t nc)
 }
 
 int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma) {
+  NvtxRange range_("hpcgx_generate");
   HANDLE(p);
   for (int l = 0; l < p->nlev; ++l) {
     if (kind == HPCGX_GEN_HPCG) {
@@ -1277,6 +1342,7 @@ int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma) {
 }
 
 int hpcgx_build_mixed(hpcgx_problem *p) {
+  NvtxRange range_("hpcgx_build_mixed");
   HANDLE(p);
   p->mixed_stale = true;
   TRY(p->check_ready(true));
@@ -1306,6 +1372,7 @@ int hpcgx_get_diagonal_host(hpcgx_problem *p, int level, double *diag) {
 }
 
 int hpcgx_set_values(hpcgx_problem *p, int level, const double *vals27, int recoarsen) {
+  NvtxRange range_("hpcgx_set_values");
   HANDLE(p);
   TRY(check_level(p, level));
   p->note(launch_set_values(p->L[level], vals27, p->stream));
@@ -1336,6 +1403,7 @@ int hpcgx_memory_bytes(hpcgx_problem *p, double *bytes) {
 }
 
 int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
+  NvtxRange range_("hpcgx_spmv");
   HANDLE(p);
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
@@ -1352,6 +1420,7 @@ int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
 }
 
 int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y) {
+  NvtxRange range_("hpcgx_spmv_stencil");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
@@ -1363,6 +1432,7 @@ int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y) 
 }
 
 int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
+  NvtxRange range_("hpcgx_symgs");
   HANDLE(p);
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
@@ -1379,6 +1449,7 @@ int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
 }
 
 int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
+  NvtxRange range_("hpcgx_mg");
   HANDLE(p);
   TRY(p->check_ready(false));
   if (p->sharded()) {
@@ -1394,6 +1465,7 @@ int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
 }
 
 int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y) {
+  NvtxRange range_("hpcgx_spmv_mixed");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
@@ -1406,6 +1478,7 @@ int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y) {
 
 int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const float *r32,
                       float *x) {
+  NvtxRange range_("hpcgx_symgs_mixed");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
@@ -1421,6 +1494,7 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
 }
 
 int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x) {
+  NvtxRange range_("hpcgx_mg_mixed");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(p->check_ready(true));
@@ -1482,6 +1556,7 @@ int hpcgx_residual(hpcgx_problem *p, int64_t n, const double *v1, const double *
 
 int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
              int precond, int *niters, double *normr, double *normr0, double *times) {
+  NvtxRange range_("hpcgx_cg");
   HANDLE(p);
   if (p->sharded()) {
     TRY(need_comm(p));
@@ -1494,6 +1569,7 @@ int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double 
 
 int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter, double tolerance,
                    int *niters, double *normr, double *normr0, double *times) {
+  NvtxRange range_("hpcgx_cg_mixed");
   HANDLE(p);
   if (p->sharded()) {
     TRY(need_comm(p));
@@ -1505,6 +1581,7 @@ int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter, d
 
 int hpcgx_cg_host(hpcgx_problem *p, int mode, const double *b_host, double *x_host, int max_iter,
                   double tolerance, int *niters, double *normr, double *normr0, double *times) {
+  NvtxRange range_("hpcgx_cg_host");
   HANDLE(p);
   const int64_t n = p->L[0].n;
   int kind;
@@ -1582,6 +1659,7 @@ int hpcgx_waxpby_host(hpcgx_problem *p, int64_t n, double alpha, const double *x
 }
 
 int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, double *grad) {
+  NvtxRange range_("hpcgx_adjoint_grad");
   HANDLE(p);
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   p->note(launch_adjoint_grad(p->L[0], lambda, x, grad, p->stream));
@@ -1661,6 +1739,7 @@ int hpcgx_nccl_unique_id(void *id, int bytes) {
 }
 
 int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
+  NvtxRange range_("hpcgx_attach_nccl");
   HANDLE(p);
   if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");
   if (p->nccl || p->comm_halo) return fail(HPCGX_ESTATE, "a communicator is attached already");
@@ -1729,6 +1808,7 @@ int hpcgx_group_destroy(hpcgx_group *g) {
 }
 
 int hpcgx_group_spmv(hpcgx_group *g, int level, const double *const *x, double *const *y) {
+  NvtxRange range_("hpcgx_group_spmv");
   if (!g || !x || !y) return fail(HPCGX_EINVAL, "null argument");
   for (hpcgx_problem *p : g->ranks) {
     TRY(check_level(p, level));
@@ -1740,6 +1820,7 @@ int hpcgx_group_spmv(hpcgx_group *g, int level, const double *const *x, double *
 }
 
 int hpcgx_group_symgs(hpcgx_group *g, int level, const double *const *r, double *const *x) {
+  NvtxRange range_("hpcgx_group_symgs");
   if (!g || !r || !x) return fail(HPCGX_EINVAL, "null argument");
   for (hpcgx_problem *p : g->ranks) {
     TRY(check_level(p, level));
@@ -1751,6 +1832,7 @@ int hpcgx_group_symgs(hpcgx_group *g, int level, const double *const *r, double 
 }
 
 int hpcgx_group_mg(hpcgx_group *g, const double *const *r, double *const *x) {
+  NvtxRange range_("hpcgx_group_mg");
   if (!g || !r || !x) return fail(HPCGX_EINVAL, "null argument");
   for (hpcgx_problem *p : g->ranks) TRY(p->check_ready(false));
   return sharded_op(g->ranks, group_runner(g), [&](hpcgx_problem *q, Plan &pl, int k) {
@@ -1760,6 +1842,7 @@ int hpcgx_group_mg(hpcgx_group *g, const double *const *r, double *const *x) {
 
 int hpcgx_group_cg(hpcgx_group *g, int mode, const double *const *b, double *const *x,
                    int max_iter, double tolerance, int *niters, double *normr, double *normr0) {
+  NvtxRange range_("hpcgx_group_cg");
   if (!g || !b || !x) return fail(HPCGX_EINVAL, "null argument");
   int kind = 0;
   TRY(group_kind(mode, &kind));

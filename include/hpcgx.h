@@ -34,6 +34,7 @@ extern "C" {
 #define HPCGX_ELAYOUT 5    /* matrix is not a 27-point stencil matrix     */
 #define HPCGX_ENOMEM 6     /* device allocation failed                    */
 #define HPCGX_ECOMM 7      /* a halo exchange or reduction across ranks failed */
+#define HPCGX_ETIMEOUT 8   /* sharded work did not finish within HPCGX_WAIT_TIMEOUT_S */
 
 #define HPCGX_GEN_HPCG 0    /* the reference problem: 26 / -1 stencil     */
 #define HPCGX_GEN_VARCOEF 1 /* variable-coefficient SPD stencil           */

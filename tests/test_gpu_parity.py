@@ -366,3 +366,11 @@ def test_error_paths(oracle):
     x.zero_()
     k, nr, nr0 = P.cg(cuda(b), x, 50, 1e-10)
     assert nr / nr0 <= 1e-10
+    # a device allocation that cannot succeed (1024^3: ~230 GB of FP64 values on
+    # the finest level alone) fails cleanly with ENOMEM before anything else is held
+    with pytest.raises(HPCGXError) as e:
+        Problem(1024, 1024, 1024)
+    assert e.value.code == 6
+    x.zero_()
+    k, nr, nr0 = P.cg(cuda(b), x, 50, 1e-10)
+    assert nr / nr0 <= 1e-10

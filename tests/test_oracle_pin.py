@@ -52,6 +52,18 @@ def test_greedy_colouring_is_parity_8_colours(case):
         assert (lev.colors == geometric_colour(lev.nx, lev.ny, lev.nz)).all()
 
 
+def test_colours_are_independent_sets(case):
+    """No two rows of one colour share a stencil edge, on every level: the rows
+    of a colour may be updated in any order (in parallel)."""
+    dims, L, b, xe, g = case
+    for lev in L:
+        rows = np.repeat(np.arange(lev.nrow), 27)
+        used = (np.arange(27)[None, :] < lev.nnz[:, None].astype(np.int64)).ravel()
+        i, j = rows[used], lev.cols.astype(np.int64)[used]
+        off = i != j
+        assert (lev.colors[i[off]] != lev.colors[j[off]]).all()
+
+
 def test_spmv_and_symgs_bitexact(case, oracle):
     dims, L, b, xe, g = case
     u, r, x0 = inputs(oracle, L[0].nrow)

@@ -90,3 +90,55 @@ def test_two_processes_exchange_through_torch_distributed(oracle):
     fx, fk, fnr, fnr0 = oracle.fcg(L, b, np.zeros(n), 500, 1e-10)
     for k in range(RANKS):
         assert out[k]["mixed"][0] == fk and out[k]["mixed"][1] <= 1e-10
+
+
+def _slow_peer(rank, out):
+    """One rank whose sum function queues ~2 s of unrelated GPU work on the
+    library's stream the first time it runs: the per-iteration wait (limit
+    0.5 s) must give up with ETIMEOUT, and the problem must work again once the
+    queued work has drained."""
+    import sys
+    os.environ["HPCGX_WAIT_TIMEOUT_S"] = "0.5"
+    sys.path.insert(0, ROOT)
+    torch.cuda.set_device(0)
+    from hpcg_b200 import HPCGXError, Problem
+    P = Problem(16, 16, 16)
+    P.generate("hpcg")
+    n = P.rows()
+    b = P.spmv(torch.ones(n, dtype=torch.float64, device="cuda"))
+    # few long launches (the launch queue of a stream is short: thousands of
+    # small ones would block the enqueueing host instead of the GPU)
+    a = torch.randn(16384, 16384, dtype=torch.bfloat16, device="cuda")
+    state = {"slow": True}
+
+    def halo(slo, rlo, shi, rhi, count, esize, stream):
+        pass                                   # one rank: never called
+
+    def sum_(buf, count, stream):
+        if state["slow"]:
+            state["slow"] = False
+            with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+                for _ in range(300):
+                    a @ a
+
+    P.attach_comm(halo, sum_)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    try:
+        P.cg(b, x, 50, 1e-10)
+        out["code"] = 0
+    except HPCGXError as e:
+        out["code"] = e.code
+    torch.cuda.synchronize()
+    x.zero_()
+    k, nr, nr0 = P.cg(b, x, 50, 1e-10)
+    out["after"] = (k, nr / nr0)
+    P.close()
+
+
+def test_bounded_wait_reports_a_stalled_rank():
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_slow_peer, args=(out,), nprocs=1, join=True, start_method="spawn")
+    assert out["code"] == 8                     # HPCGX_ETIMEOUT
+    k, rel = out["after"]
+    assert rel <= 1e-10
