@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libhpcgx.so")
+# HPCGX_LIBRARY=checked selects the index-checked build (libhpcgx_checked.so)
+LIB_PATH = os.path.join(HERE, "libhpcgx_checked.so" if os.environ.get("HPCGX_LIBRARY") == "checked"
+                        else "libhpcgx.so")
 
 _P = C.c_void_p
 _I = C.c_int
@@ -76,6 +78,7 @@ SIGNATURES = {
     "hpcgx_nccl_unique_id": (_I, [_P, _I]),
     "hpcgx_attach_nccl": (_I, [_P, _P, _I]),
     "hpcgx_attach_comm": (_I, [_P, HALO_FN, SUM_FN, _P]),
+    "hpcgx_check_status": (_I, []),
     "hpcgx_group_create": (_I, [_P, _I, C.POINTER(_P)]),
     "hpcgx_group_destroy": (_I, [_P]),
     "hpcgx_group_spmv": (_I, [_P, _I, _P, _P]),
@@ -86,7 +89,7 @@ SIGNATURES = {
 
 HPCGX_OK = 0
 ERRORS = {1: "EINVAL", 2: "ECUDA", 3: "ESTATE", 4: "ENONFINITE", 5: "ELAYOUT", 6: "ENOMEM",
-          7: "ECOMM", 8: "ETIMEOUT"}
+          7: "ECOMM", 8: "ETIMEOUT", 9: "ECHECK"}
 NCCL_ID_BYTES = 128
 GEN_HPCG, GEN_VARCOEF = 0, 1
 PROBE_NONE, PROBE_GS_FINE, PROBE_SPMV_FINE, PROBE_GS_FINE_BWD = 0, 1, 2, 4

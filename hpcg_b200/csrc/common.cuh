@@ -84,6 +84,7 @@ struct LevelMat {
   // the index range [lo, lo + span) of the vector including them
   int zlo, zhi;
   int lo, span;
+  int64_t srows;   // storage rows (colours padded to 32)
   // Stencil offsets: slot s of row i holds column i + off[s] whenever the row
   // has that neighbour (the layout enforces it when a level is loaded), and
   // column i with value 0 otherwise.  The mixed-precision V-cycle and the

@@ -226,6 +226,38 @@ __global__ void k_rank_sum(int nranks, double *const *bufs, int count) {
   }
 }
 
+// ---------------------------------------------------------------- index checks
+
+// Built with -DHPCGX_CHECKED (libhpcgx_checked.so), the row kernels verify
+// every storage row, vector row and gathered column before using it; a bad
+// one is recorded (the first, as site << 56 | index) and replaced by index 0,
+// which is always inside the buffers, so nothing outside them is touched.
+// hpcgx_check_status() reports and clears the record.  The stand-in for a
+// memory checker; without the macro the checks compile to nothing.
+#ifdef HPCGX_CHECKED
+__device__ unsigned long long g_check_record = 0ull;
+__device__ __noinline__ void check_fail(int site, int64_t index) {
+  atomicCAS(&g_check_record, 0ull,
+            ((unsigned long long)site << 56) | ((unsigned long long)index & ((1ull << 56) - 1)));
+}
+#endif
+
+struct RowId;
+template <class VT>
+__device__ __forceinline__ void check_row(const LevelMat<VT> &A, RowId &id, int site);
+template <class VT, class NEED>
+__device__ __forceinline__ void check_cols(const LevelMat<VT> &A, int32_t *col, NEED need,
+                                           int site);
+__device__ __forceinline__ int64_t check_index(int64_t i, int64_t n, int site) {
+#ifdef HPCGX_CHECKED
+  if (i < 0 || i >= n) {
+    check_fail(site, i);
+    return 0;
+  }
+#endif
+  return i;
+}
+
 // ---------------------------------------------------------------- geometry
 
 struct ClassSet {
@@ -265,6 +297,33 @@ struct RowId {
   int64_t k;     // storage row
   int ix, iy, iz;
 };
+
+template <class VT>
+__device__ __forceinline__ void check_row(const LevelMat<VT> &A, RowId &id, int site) {
+#ifdef HPCGX_CHECKED
+  if (id.row < 0 || id.row >= A.n) {
+    check_fail(site, id.row);
+    id.row = 0;
+  }
+  if (id.k < 0 || id.k >= A.srows) {
+    check_fail(site, id.k);
+    id.k = 0;
+  }
+#endif
+}
+
+template <class VT, class NEED>
+__device__ __forceinline__ void check_cols(const LevelMat<VT> &A, int32_t *col, NEED need,
+                                           int site) {
+#ifdef HPCGX_CHECKED
+#pragma unroll
+  for (int s = 0; s < HPCGX_STENCIL; ++s)
+    if (need(s) && (uint32_t)(col[s] - A.lo) >= (uint32_t)A.span) {
+      check_fail(site, col[s]);
+      col[s] = 0;
+    }
+#endif
+}
 
 __device__ __forceinline__ RowId row_of(const ClassInfo &C, int nx, int ny, int px, int j0,
                                         int t) {
@@ -446,7 +505,8 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
   for (int px = 0; px < 2; ++px) {
     const int cnt = (j1 - j0) * C.len[px];
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-      const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
+      RowId id = row_of(C, A.nx, A.ny, px, j0, t);
+      check_row(A, id, 1);
       int32_t col[HPCGX_STENCIL];
       VT val[HPCGX_STENCIL];
 #pragma unroll
@@ -455,6 +515,7 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
         load_plane(A.vals, id.k, p, NeedAll(), val + 9 * p);
       }
       if (IMPL) stencil_cols<false>(A, id, NeedAll(), col);
+      check_cols(A, col, NeedAll(), 2);
       T xv[HPCGX_STENCIL];
 #pragma unroll
       for (int s = 0; s < HPCGX_STENCIL; ++s) xv[s] = __ldg(x + col[s]);
@@ -493,9 +554,11 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 //       the two only x_i changes, so the backward value is recomputed from the
 //       same registers and only that value is stored.
 template <bool ZERO, bool PRO, bool RES, bool SYM = false, class VT, class T, class RT>
-__device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, int c,
+__device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, int c,
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
                                        T *__restrict__ rc) {
+  RowId id = id0;
+  check_row(A, id, 3);
   int32_t col[HPCGX_STENCIL];
   T val[HPCGX_STENCIL];   // values converted to the arithmetic type as loaded
   // slots whose neighbour is read: all, or (zero guess) the lower colours
@@ -509,11 +572,13 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id, i
     if (!IMPLICIT) load_plane(A.cols, id.k, p, need, col + 9 * p);
   }
   if (IMPLICIT) stencil_cols<true>(A, id, need, col);
+  check_cols(A, col, need, 4);
   const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
   if (PRO || RES) {
     const int nxc = A.nx >> 1, nyc = A.ny >> 1;
     crow = ((int64_t)(id.iz >> 1) * nyc + (id.iy >> 1)) * nxc + (id.ix >> 1);
+    crow = check_index(crow, (int64_t)nxc * nyc * (A.nz >> 1), 5);
   }
   T xi = ZERO ? T(0) : x[id.row];
   if (PRO) xi = rn_add(xi, __ldg(xc + crow));
@@ -658,6 +723,7 @@ k_restrict_residual(LevelMat<VT> A, ClassInfo C0, int64_t nc, const RT *__restri
     id.iz = 2 * izc;
     id.row = ((int64_t)id.iz * A.ny + id.iy) * A.nx + id.ix;
     id.k = C0.start[0] + ((int64_t)izc * C0.nyq + iyc) * C0.len[0] + ixc;  // colour 0
+    check_row(A, id, 6);
     int32_t col[HPCGX_STENCIL];
     T val[HPCGX_STENCIL];
 #pragma unroll
@@ -666,6 +732,7 @@ k_restrict_residual(LevelMat<VT> A, ClassInfo C0, int64_t nc, const RT *__restri
       if (!IMPLICIT) load_plane(A.cols, id.k, p, NeedAll(), col + 9 * p);
     }
     if (IMPLICIT) stencil_cols<true>(A, id, NeedAll(), col);
+    check_cols(A, col, NeedAll(), 7);
     T ax = T(0);
 #pragma unroll
     for (int s = 0; s < HPCGX_STENCIL; ++s) ax = mac_add(ax, val[s], x[col[s]]);
@@ -1121,6 +1188,7 @@ LevelMat<VT> mat_of(const LevelDev &L, const VT *vals) {
   A.zhi = L.zhi;
   A.lo = L.zlo ? -L.nx * L.ny : 0;
   A.span = (int)L.n - A.lo + (L.zhi ? L.nx * L.ny : 0);
+  A.srows = L.storage_rows;
   return A;
 }
 
@@ -1362,6 +1430,18 @@ template int launch_prolong<double>(const LevelDev &, int64_t, const double *, d
                                     const int *, cudaStream_t);
 template int launch_prolong<float>(const LevelDev &, int64_t, const float *, float *, const int *,
                                    cudaStream_t);
+
+int read_check_record(unsigned long long *record) {
+  *record = 0ull;
+#ifdef HPCGX_CHECKED
+  cudaError_t e = cudaMemcpyFromSymbol(record, g_check_record, sizeof(*record));
+  if (e != cudaSuccess) return (int)e;
+  const unsigned long long zero = 0ull;
+  e = cudaMemcpyToSymbol(g_check_record, &zero, sizeof(zero));
+  if (e != cudaSuccess) return (int)e;
+#endif
+  return 0;
+}
 
 int launch_finish(int fin, int nv, const double *tot, CgState *st, cudaStream_t s) {
   if (nv == 2)

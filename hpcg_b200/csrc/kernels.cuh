@@ -113,6 +113,10 @@ int launch_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double *v, cud
 // CG pieces ---------------------------------------------------------------
 int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, const Reduce &red,
                     CgState *st, cudaStream_t s);
+// Index-check record of a -DHPCGX_CHECKED build (0 = clean; else site << 56 |
+// index of the first bad index), cleared by reading; always 0 otherwise.
+// Returns a cudaError_t value.
+int read_check_record(unsigned long long *record);
 // The scalar step `fin` on nv totals (a deferred reduction, summed over ranks).
 int launch_finish(int fin, int nv, const double *tot, CgState *st, cudaStream_t s);
 // bufs: device array of nranks pointers to `count` doubles each; every buffer

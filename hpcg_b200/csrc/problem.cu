@@ -1727,6 +1727,21 @@ int hpcgx_synchronize(hpcgx_problem *p) {
   return HPCGX_OK;
 }
 
+int hpcgx_check_status(void) {
+  CK(cudaDeviceSynchronize());
+  unsigned long long rec = 0ull;
+  const int e = read_check_record(&rec);
+  if (e != 0) return cuda_fail((cudaError_t)e);
+  if (rec == 0ull) return HPCGX_OK;
+  static const char *sites[] = {"?", "SpMV row", "SpMV column", "Gauss-Seidel row",
+                                "Gauss-Seidel column", "coarse row", "restriction row",
+                                "restriction column"};
+  const int site = (int)(rec >> 56);
+  const long long index = (long long)(rec & ((1ull << 56) - 1));
+  return fail(HPCGX_ECHECK, std::string("index check: ") + (site < 8 ? sites[site] : "?") +
+                                " index " + std::to_string(index) + " out of range");
+}
+
 // ---- sharding
 int hpcgx_nccl_unique_id(void *id, int bytes) {
   if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");

@@ -351,6 +351,12 @@ class Problem:
         check(lib().hpcgx_synchronize(self.h))
 
 
+def check_status() -> None:
+    """Raises HPCGXError(ECHECK) if a kernel of the index-checked build
+    (HPCGX_LIBRARY=checked) met an out-of-range index since the last call."""
+    check(lib().hpcgx_check_status())
+
+
 def nccl_unique_id() -> bytes:
     """A fresh NCCL unique id (rank 0 makes it; every rank attaches with it)."""
     buf = C.create_string_buffer(_lib.NCCL_ID_BYTES)

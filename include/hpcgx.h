@@ -35,6 +35,7 @@ extern "C" {
 #define HPCGX_ENOMEM 6     /* device allocation failed                    */
 #define HPCGX_ECOMM 7      /* a halo exchange or reduction across ranks failed */
 #define HPCGX_ETIMEOUT 8   /* sharded work did not finish within HPCGX_WAIT_TIMEOUT_S */
+#define HPCGX_ECHECK 9     /* index-checked build: a kernel met an out-of-range index */
 
 #define HPCGX_GEN_HPCG 0    /* the reference problem: 26 / -1 stencil     */
 #define HPCGX_GEN_VARCOEF 1 /* variable-coefficient SPD stencil           */
@@ -220,6 +221,12 @@ int hpcgx_probe_read(hpcgx_problem *p, int kind, double *ms, int64_t *launches, 
 int64_t hpcgx_launch_count(hpcgx_problem *p);
 /* Waits for all work of the problem's stream. */
 int hpcgx_synchronize(hpcgx_problem *p);
+/* Index-checked build (libhpcgx_checked.so, compiled with -DHPCGX_CHECKED):
+ * HPCGX_ECHECK if a kernel has met an out-of-range storage row, vector row
+ * or column since the last call (the first one is named in the message; the
+ * access itself was redirected into the buffers), else HPCGX_OK.  Synchronises
+ * the device.  Always HPCGX_OK in the regular build, which has no checks. */
+int hpcgx_check_status(void);
 
 /* ---- sharding over ranks (z-slabs) --------------------------------------
  * The reference's MPI decomposition with a process grid of 1 x 1 x nranks

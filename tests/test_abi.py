@@ -36,6 +36,18 @@ def test_library_exports_every_declared_symbol():
     assert h.hpcgx_version() >= 1
 
 
+def test_checked_library_exports_the_same_symbols():
+    """The index-checked build (HPCGX_LIBRARY=checked) is the same ABI."""
+    import ctypes
+    from hpcg_b200 import _lib
+    path = os.path.join(_lib.HERE, "libhpcgx_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("libhpcgx_checked.so not built")
+    h = ctypes.CDLL(path)
+    for name in declared():
+        assert hasattr(h, name), name
+
+
 def test_library_is_sm100a_only():
     """The fatbin is built for sm_100a (checked from the build recipe, not by
     reading the binary)."""
