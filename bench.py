@@ -597,9 +597,10 @@ def main():
 
 # Iterations the reference arm scales its per-iteration sample to when run on
 # its own: the FP64 PCG iteration count this build measured on the same
-# system (recorded by bench runs; the reference's natural-order smoother is
-# not run at 512^3 because its int32 counters overflow there).
-REF_ITERS_DEFAULT = {}
+# system to 1e-10 (bench runs on B200: 295 at 512^3, 170 at 256^3); the
+# reference's natural-order smoother is not run at 512^3 because its int32
+# counters overflow there.
+REF_ITERS_DEFAULT = {(512, 512, 512): 295, (256, 256, 256): 170}
 
 
 if __name__ == "__main__":
