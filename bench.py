@@ -555,7 +555,7 @@ def main():
             dist.destroy_process_group()
         return
     cpu = None
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:   # the CPU sample is taken at N = 1 only
         try:
             cpu = cpu_reference_sample(k64, dims)
         except Exception as e:  # the baseline is reported, never required
