@@ -546,9 +546,14 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 //       (first forward sweep after ZeroVector); those terms, and the padding
 //       slots (column = row), are skipped.  Skipping a product with a zero
 //       changes nothing but possibly the sign of an exact zero.
-// PRO:  x_i first receives the prolongated coarse correction (colour 0).
+// PRO:  x_i first receives the prolongated coarse correction (colour 0) --
+//       except in the first plane of a slab with a halo below, whose
+//       correction is added before the halo exchange (the slab below reads
+//       that plane).
 // RES:  after the update, the fine residual at this injected point is formed
 //       and restricted: rc = r_i - (A x)_i with (A x)_i summed as in SpMV.
+//       (A slab with a halo below forms its first plane's again once the
+//       halo holds the slab below's smoothed values.)
 // SYM:  forward update of a row of the last colour, immediately followed by
 //       its backward update (the first step of the backward sweep): between
 //       the two only x_i changes, so the backward value is recomputed from the
@@ -581,7 +586,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
     crow = check_index(crow, (int64_t)nxc * nyc * (A.nz >> 1), 5);
   }
   T xi = ZERO ? T(0) : x[id.row];
-  if (PRO) xi = rn_add(xi, __ldg(xc + crow));
+  if (PRO && !(A.zlo && id.iz == 0)) xi = rn_add(xi, __ldg(xc + crow));
   // A slot without a neighbour holds value 0 and the row itself as column; in
   // the zero-guess sweep x_i is unwritten, so that term -- a product with 0 --
   // is skipped below.  The gather itself does not wait for the value: every
@@ -705,7 +710,8 @@ k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, 
 // ComputeSPMV_ref does (src/ComputeSPMV_ref.cpp:64-70), then
 // src/ComputeRestriction_ref.cpp:51.  The standalone form of GS_RESTRICT, for
 // the sharded V-cycle, where the halo of x is exchanged between the sweep and
-// the residual (src/ComputeMG_ref.cpp:49-51).
+// the residual (src/ComputeMG_ref.cpp:49-51): launched over the first coarse
+// plane only (nc = nxc * nyc), the one injected plane that reads the halo.
 template <class VT, class T, class RT>
 __global__ void __launch_bounds__(kThreads)
 k_restrict_residual(LevelMat<VT> A, ClassInfo C0, int64_t nc, const RT *__restrict__ rf,
@@ -741,7 +747,8 @@ k_restrict_residual(LevelMat<VT> A, ClassInfo C0, int64_t nc, const RT *__restri
 }
 
 // xf += xc at the injected points (src/ComputeProlongation_ref.cpp:49), in the
-// vector type of the V-cycle.
+// vector type of the V-cycle.  The sharded V-cycle launches it over the first
+// coarse plane only, before the halo exchange; GS_PROLONG adds the rest.
 template <class T>
 __global__ void __launch_bounds__(kThreads)
 k_prolong(int64_t nc, int nxf, int nyf, const T *__restrict__ xc, T *xf,
@@ -1402,27 +1409,29 @@ int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *
 }
 
 template <class T, class RT>
-int launch_restrict_residual(const LevelDev &F, const RT *rf, const T *xf, T *rc, const int *done,
-                             cudaStream_t s) {
-  const int64_t nc = (int64_t)(F.nx / 2) * (F.ny / 2) * (F.nz / 2);
-  if (nc == 0) return 0;
+int launch_restrict_residual(const LevelDev &F, int64_t nc, const RT *rf, const T *xf, T *rc,
+                             const int *done, cudaStream_t s) {
+  if (nc <= 0) return 0;
+  nc = std::min(nc, (int64_t)(F.nx / 2) * (F.ny / 2) * (F.nz / 2));
   k_restrict_residual<<<grid_for(nc), kThreads, 0, s>>>(mat_of(F, ValsOf<T>::get(F)), F.cls[0],
                                                         nc, rf, xf, rc, done);
   return 1;
 }
-template int launch_restrict_residual<double, double>(const LevelDev &, const double *,
+template int launch_restrict_residual<double, double>(const LevelDev &, int64_t, const double *,
                                                       const double *, double *, const int *,
                                                       cudaStream_t);
-template int launch_restrict_residual<float, double>(const LevelDev &, const double *,
+template int launch_restrict_residual<float, double>(const LevelDev &, int64_t, const double *,
                                                      const float *, float *, const int *,
                                                      cudaStream_t);
-template int launch_restrict_residual<float, float>(const LevelDev &, const float *, const float *,
-                                                    float *, const int *, cudaStream_t);
+template int launch_restrict_residual<float, float>(const LevelDev &, int64_t, const float *,
+                                                    const float *, float *, const int *,
+                                                    cudaStream_t);
 
 template <class T>
 int launch_prolong(const LevelDev &F, int64_t nc, const T *xc, T *xf, const int *done,
                    cudaStream_t s) {
-  if (nc == 0) return 0;
+  if (nc <= 0) return 0;
+  nc = std::min(nc, (int64_t)(F.nx / 2) * (F.ny / 2) * (F.nz / 2));
   k_prolong<T><<<grid_for(nc), kThreads, 0, s>>>(nc, F.nx, F.ny, xc, xf, done);
   return 1;
 }

@@ -124,11 +124,12 @@ int launch_finish(int fin, int nv, const double *tot, CgState *st, cudaStream_t 
 int launch_rank_sum(int nranks, double *const *bufs, int count, cudaStream_t s);
 // Standalone restriction of the residual at the injected points,
 // rc = rf - (A x) there (src/ComputeSPMV_ref.cpp + src/ComputeRestriction_ref.cpp:51),
-// and prolongation xf += xc at the injected points; used where a halo
-// exchange separates them from the sweeps.
+// and prolongation xf += xc at the injected points, over the first nc coarse
+// points (coarse row order); used where a halo exchange separates them from
+// the sweeps.
 template <class T, class RT>
-int launch_restrict_residual(const LevelDev &F, const RT *rf, const T *xf, T *rc, const int *done,
-                             cudaStream_t s);
+int launch_restrict_residual(const LevelDev &F, int64_t nc, const RT *rf, const T *xf, T *rc,
+                             const int *done, cudaStream_t s);
 template <class T>
 int launch_prolong(const LevelDev &F, int64_t nc, const T *xc, T *xf, const int *done,
                    cudaStream_t s);

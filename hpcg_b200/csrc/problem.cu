@@ -554,28 +554,42 @@ struct hpcgx_problem {
     return HPCGX_OK;
   }
   // One symmetric sweep of level l (7 class launches) after the halo of x.
+  // xc: the first forward class adds the prolongated correction (GS_PROLONG);
+  // rc: the last backward class forms the restricted residual (GS_RESTRICT).
   template <class T, class RT>
-  void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done) {
+  void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done,
+                   const T *xc = nullptr, T *rc = nullptr) {
     const int m0 = zero ? GS_ZERO_GUESS : GS_PLAIN;
-    for (int q = 0; q < 3; ++q)
+    for (int q = 0; q < 3; ++q) {
+      const int m = (q == 0 && xc) ? GS_PROLONG : m0;
       add(pl, [=]() {
-        note(launch_gs_class<T, RT>(L[l], q, 0, m0, r, x, nullptr, nullptr, done, stream));
+        note(launch_gs_class<T, RT>(L[l], q, 0, m, r, x, xc, nullptr, done, stream));
         return HPCGX_OK;
       });
+    }
     add(pl, [=]() {
       note(launch_gs_class<T, RT>(L[l], 3, 0, GS_SYM3 | m0, r, x, nullptr, nullptr, done, stream));
       return HPCGX_OK;
     });
-    for (int q = 2; q >= 0; --q)
+    for (int q = 2; q >= 0; --q) {
+      const int m = (q == 0 && rc) ? GS_RESTRICT : GS_PLAIN;
       add(pl, [=]() {
-        note(launch_gs_class<T, RT>(L[l], q, 1, GS_PLAIN, r, x, nullptr, nullptr, done, stream));
+        note(launch_gs_class<T, RT>(L[l], q, 1, m, r, x, nullptr, rc, done, stream));
         return HPCGX_OK;
       });
+    }
   }
-  // The V-cycle of src/ComputeMG_ref.cpp:39-63 on a z-slab: restriction and
-  // prolongation are separate launches, since the reference exchanges the
-  // halo of x between the pre-smoother and the residual and between the
-  // prolongation and the post-smoother.  x0 must be a haloed vector.
+  // The V-cycle of src/ComputeMG_ref.cpp:39-63 on a z-slab.  The reference
+  // exchanges the halo of x between the pre-smoother and the residual and
+  // between the prolongation and the post-smoother.  Only the first plane of
+  // a slab (even z, injected) reads the halo below, and no injected point
+  // reads the halo above (the local z-extent is even), so restriction and
+  // prolongation stay fused into the sweeps and two one-plane launches
+  // restore the reference's order there: after the exchange that follows the
+  // pre-smoother, the first plane's residual is formed again; before the
+  // exchange that precedes the post-smoother, the first plane receives its
+  // correction (which the fused prolongation then skips).  x0 must be a
+  // haloed vector.
   template <class T, class RT0>
   void plan_vcycle(Plan &pl, const RT0 *r0, T *x0, const int *done) {
     T *xl[kMaxLevels];
@@ -583,22 +597,25 @@ struct hpcgx_problem {
     auto rl = [&](int l) { return lvl_r(L[l], (T *)nullptr); };
     for (int l = 0; l + 1 < nlev; ++l) {
       T *x = xl[l];
+      T *rc = rl(l + 1);
       add(pl, [=]() { return zero_halo<T>(l, x); });
       if (l == 0)
-        plan_sweeps<T, RT0>(pl, 0, r0, x, true, done);
+        plan_sweeps<T, RT0>(pl, 0, r0, x, true, done, nullptr, rc);
       else
-        plan_sweeps<T, T>(pl, l, rl(l), x, true, done);
+        plan_sweeps<T, T>(pl, l, rl(l), x, true, done, nullptr, rc);
       add_halo(pl, l, x, sizeof(T));
-      T *rc = rl(l + 1);
+      // (every rank plans the same steps; the one-plane launches are empty
+      //  on a slab without a halo below)
+      const int64_t plane_c = L[l].zlo ? (int64_t)L[l + 1].nx * L[l + 1].ny : 0;
       if (l == 0)
         add(pl, [=]() {
-          note(launch_restrict_residual<T, RT0>(L[0], r0, x, rc, done, stream));
+          note(launch_restrict_residual<T, RT0>(L[0], plane_c, r0, x, rc, done, stream));
           return HPCGX_OK;
         });
       else {
         const T *rf = rl(l);
         add(pl, [=]() {
-          note(launch_restrict_residual<T, T>(L[l], rf, x, rc, done, stream));
+          note(launch_restrict_residual<T, T>(L[l], plane_c, rf, x, rc, done, stream));
           return HPCGX_OK;
         });
       }
@@ -615,16 +632,16 @@ struct hpcgx_problem {
     for (int l = nlev - 2; l >= 0; --l) {
       T *x = xl[l];
       const T *xc = xl[l + 1];
-      const int64_t nc = L[l + 1].n;
+      const int64_t plane_c = L[l].zlo ? (int64_t)L[l + 1].nx * L[l + 1].ny : 0;
       add(pl, [=]() {
-        note(launch_prolong<T>(L[l], nc, xc, x, done, stream));
+        note(launch_prolong<T>(L[l], plane_c, xc, x, done, stream));
         return HPCGX_OK;
       });
       add_halo(pl, l, x, sizeof(T));
       if (l == 0)
-        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done);
+        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc);
       else
-        plan_sweeps<T, T>(pl, l, rl(l), x, false, done);
+        plan_sweeps<T, T>(pl, l, rl(l), x, false, done, xc);
     }
   }
   // The haloed staging vector of level l (operator inputs arrive without halo).
