@@ -636,33 +636,18 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
   }
 }
 
-// A half sweep over one class: colours 2q then 2q+1 (forward, DIR = 0) or
-// 2q+1 then 2q (backward, DIR = 1).  MODE bits: GS_ZERO_GUESS for the whole
-// launch; GS_PROLONG and GS_RESTRICT act on colour 0 only.  QS >= 0 fixes the
-// class at compile time, which lets the zero-guess sweep drop the loads of the
-// skipped slots statically.
-// Occupancy: the FP64 sweeps stream 12 B per slot and saturate HBM with two
-// 256-thread blocks per SM; the BF16 sweeps read 2 B per slot and are latency
-// bound, so they are held to 64 registers for four blocks per SM (five,
-// at 48 registers, spill and run slower).
-template <class VT>
-constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 4 : 2; }
-
-template <int MODE, int DIR, int QS, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
-k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
-  if (done && *done) return;
-  constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0;
-  constexpr bool PRO = (MODE & GS_PROLONG) != 0;
-  constexpr bool RES = (MODE & GS_RESTRICT) != 0;
-  const int q = QS >= 0 ? QS : C.q;
-  const int j0 = blockIdx.x * lpb;
-  const int j1 = min(j0 + lpb, C.lines);
+// One half sweep of class Q over the lines [j0, j1) of the class: colours
+// 2Q then 2Q+1 (DIR = 0) or 2Q+1 then 2Q (DIR = 1).  A block owns whole lines,
+// so the x-neighbours of a row (the other colour of the class) are its own.
+// PRO / RES act on colour 0 only.
+template <bool ZERO, bool PRO, bool RES, int Q, int DIR, class VT, class T, class RT>
+__device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo &C, int j0, int j1,
+                                         const RT *__restrict__ r, T *x,
+                                         const T *__restrict__ xc, T *__restrict__ rc) {
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
     const int px = DIR ? 1 - half : half;
-    const int c = px + 2 * q;
+    const int c = px + 2 * (Q >= 0 ? Q : C.q);
     const int cnt = (j1 - j0) * C.len[px];
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
       const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
@@ -676,18 +661,15 @@ k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
 }
 
 // The last class of a forward sweep fused with the first class of the
-// following backward sweep: colour 6 forward, colour 7 forward and backward
-// (SYM), colour 6 backward.  Class 3's colours only depend on each other
-// along x inside a line, so the block's own lines carry every dependency;
-// the matrix rows of the class are read from DRAM once instead of twice
-// (colour 6's rows come back from L2 in the last phase).
+// following backward sweep, over the lines [j0, j1) of class 3: colour 6
+// forward, colour 7 forward and backward (SYM), colour 6 backward.  Class 3's
+// colours only depend on each other along x inside a line, so the block's own
+// lines carry every dependency; the matrix rows of the class are read from
+// DRAM once instead of twice (colour 6's rows come back from L2 in the last
+// phase).
 template <bool ZERO, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
-k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-                const int *__restrict__ done) {
-  if (done && *done) return;
-  const int j0 = blockIdx.x * lpb;
-  const int j1 = min(j0 + lpb, C.lines);
+__device__ __forceinline__ void gs_lines_sym3(const LevelMat<VT> &A, const ClassInfo &C, int j0,
+                                              int j1, const RT *__restrict__ r, T *x) {
   const int cnt0 = (j1 - j0) * C.len[0], cnt1 = (j1 - j0) * C.len[1];
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
     gs_row<ZERO, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
@@ -703,6 +685,201 @@ k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, 
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
     gs_row<false, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
                                 (T *)nullptr);
+}
+
+// A half sweep over one class, lpb lines per block.  MODE bits:
+// GS_ZERO_GUESS for the whole launch; GS_PROLONG and GS_RESTRICT act on
+// colour 0 only.  QS >= 0 fixes the class at compile time, which lets the
+// zero-guess sweep drop the loads of the skipped slots statically.
+// Occupancy: the FP64 sweeps stream 12 B per slot and saturate HBM with two
+// 256-thread blocks per SM; the BF16 sweeps read 2 B per slot and are latency
+// bound, so they are held to 64 registers for four blocks per SM (five,
+// at 48 registers, spill and run slower).
+template <class VT>
+constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 4 : 2; }
+
+template <int MODE, int DIR, int QS, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
+k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
+           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
+  if (done && *done) return;
+  const int j0 = blockIdx.x * lpb;
+  const int j1 = min(j0 + lpb, C.lines);
+  gs_lines<(MODE & GS_ZERO_GUESS) != 0, (MODE & GS_PROLONG) != 0, (MODE & GS_RESTRICT) != 0, QS,
+           DIR>(A, C, j0, j1, r, x, xc, rc);
+}
+
+template <bool ZERO, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
+k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
+                const int *__restrict__ done) {
+  if (done && *done) return;
+  const int j0 = blockIdx.x * lpb;
+  const int j1 = min(j0 + lpb, C.lines);
+  gs_lines_sym3<ZERO>(A, C, j0, j1, r, x);
+}
+
+// ---------------------------------------------------------------- one-launch sweep
+//
+// A whole symmetric sweep of one level in one launch.  The seven class steps
+// of the class launches -- forward classes 0, 1, 2, class 3 forward and
+// backward, backward classes 2, 1, 0 -- become stages 0..6 of a wavefront
+// over the z-planes.  A work item is a run of lines of one stage's class in
+// one z-plane (classes 0 and 1 live on even planes, 2 and 3 on odd ones).
+//
+// Order: stage s may start plane z once stage s-1 has finished every one of
+// the planes z-1, z, z+1 that holds its class.  Then every earlier stage has
+// finished those planes (by induction), so the rows the item reads hold the
+// values they hold in the class launches: a row of an earlier colour its new
+// value, a row of a later colour its old one, since a later stage reaches a
+// plane next to z only after this stage finished z.  Within a colour the
+// rows are independent, so the sweep is bit-identical to the class launches.
+//
+// Scheduling: items carry tickets sorted by key = z + lag * s (lag >= 2), so
+// every item an item waits for has a smaller ticket.  Blocks take tickets
+// from a counter and only wait for tickets already taken by running blocks;
+// the waits end whatever the number of co-resident blocks.  A finished item
+// adds one to its (stage, plane) counter with release semantics; a waiting
+// block's first thread reads the counters with acquire semantics, then the
+// block synchronises, so the whole block sees the finished rows.  Every wait
+// gives up after kWaveSpin polls, records a fault (read by the host) and
+// stops the launch's remaining items.  The last block to leave resets the
+// counters for the next launch.
+//
+// What it is for: each class launch reads the x-neighbourhood of its rows in
+// all z-planes, i.e. the whole x vector, from DRAM; the wavefront keeps the
+// few planes between its first and last stage in L2, so x and the right-hand
+// side pass through DRAM about once per sweep instead of once per step.
+// Measured on B200 at 512^3 (mixed V-cycle, finest level) it is slower than
+// the class launches all the same -- 3.79 ms per symmetric sweep at lag 6 and
+// 2048-row items against 3.32 ms, the lag hardly mattering -- so it is an
+// option (HPCGX_GS_WAVE=1), not the default.
+
+struct WaveDev {
+  const int2 *tab;   // (stage << 16 | class plane, first ticket), ticket order
+  int *ctr;          // [7][nzq] finished items; then ticket, exits, abort
+  int ntab, total, lpi, nzq, nz;
+  int ipp[4];        // items per plane of each class
+  int uniform;       // > 0: every entry has this many items (entry = ticket / uniform)
+};
+
+__device__ unsigned int g_wave_fault = 0u;
+constexpr int kWaveSpin = 1 << 22;
+constexpr int kWaveSmemEntries = 4096;   // 16 KB of shared memory per block at most
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void red_release_gpu(int *p, int v) {
+  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__host__ __device__ constexpr int wave_class(int s) { return s <= 3 ? s : 6 - s; }
+
+// First thread only: waits until stage s-1 has finished the planes next to iz.
+__device__ bool wave_wait(const WaveDev &W, int s, int iz) {
+  const int p = s - 1, qp = wave_class(p), pzp = qp >> 1;
+  const int need = qp == 0 ? W.ipp[0] : qp == 1 ? W.ipp[1] : qp == 2 ? W.ipp[2] : W.ipp[3];
+  int *abortf = W.ctr + 7 * W.nzq + 2;
+  for (int z = iz - 1; z <= iz + 1; ++z) {
+    if (z < 0 || z >= W.nz || (z & 1) != pzp) continue;
+    const int *c = W.ctr + p * W.nzq + ((z - pzp) >> 1);
+    for (int polls = 0; ld_acquire_gpu(c) < need; ++polls) {
+      if (polls >= kWaveSpin) atomicOr(&g_wave_fault, 1u);
+      if (polls >= kWaveSpin || *(volatile int *)abortf) {
+        atomicExch(abortf, 1);
+        return false;
+      }
+      __nanosleep(128);
+    }
+  }
+  return true;
+}
+
+template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
+k_gs_wave(LevelMat<VT> A, ClassSet CS, WaveDev W, const RT *__restrict__ r, T *x,
+          const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
+  if (done && *done) return;
+  __shared__ int item[3];
+  // uniform tables are decoded from shared memory: entry = ticket / uniform
+  extern __shared__ int tab_code[];
+  const bool stab = W.uniform > 0 && W.ntab <= kWaveSmemEntries;
+  if (stab) {
+    for (int i = threadIdx.x; i < W.ntab; i += blockDim.x) tab_code[i] = W.tab[i].x;
+    __syncthreads();
+  }
+  int *ticket = W.ctr + 7 * W.nzq;
+  // The first thread holds the ticket of the next item while the block works
+  // on the current one, so that the atomic's latency is hidden (the held
+  // ticket is larger than the current one, which never waits for it).
+  int next = 0;
+  if (threadIdx.x == 0) next = atomicAdd(ticket, 1);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int s = -1, jz = 0, b = 0;
+      const int t = next;
+      if (t < W.total && !*(volatile int *)(ticket + 2)) {
+        int2 e;
+        if (stab) {
+          const int i = t / W.uniform;
+          e = make_int2(tab_code[i], i * W.uniform);
+        } else if (W.uniform > 0) {
+          e = W.tab[t / W.uniform];
+        } else {
+          int lo = 0, hi = W.ntab - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (W.tab[mid].y <= t) lo = mid; else hi = mid - 1;
+          }
+          e = W.tab[lo];
+        }
+        s = e.x >> 16;
+        jz = e.x & 0xffff;
+        b = t - e.y;
+        if (s > 0 && !wave_wait(W, s, (wave_class(s) >> 1) + 2 * jz)) s = -1;
+        if (s >= 0) next = atomicAdd(ticket, 1);
+      }
+      item[0] = s;
+      item[1] = jz;
+      item[2] = b;
+    }
+    __syncthreads();
+    const int s = item[0], jz = item[1], b = item[2];
+    if (s < 0) break;
+    const int nyq = s == 0 || s == 6 ? CS.c[0].nyq : s == 1 || s == 5 ? CS.c[1].nyq
+                  : s == 2 || s == 4 ? CS.c[2].nyq : CS.c[3].nyq;
+    const int j0 = jz * nyq + b * W.lpi;
+    const int j1 = min(j0 + W.lpi, (jz + 1) * nyq);
+    switch (s) {
+      case 0: gs_lines<ZERO, PRO, false, 0, 0>(A, CS.c[0], j0, j1, r, x, xc, rc); break;
+      case 1: gs_lines<ZERO, false, false, 1, 0>(A, CS.c[1], j0, j1, r, x, xc, rc); break;
+      case 2: gs_lines<ZERO, false, false, 2, 0>(A, CS.c[2], j0, j1, r, x, xc, rc); break;
+      case 3: gs_lines_sym3<ZERO>(A, CS.c[3], j0, j1, r, x); break;
+      case 4: gs_lines<false, false, false, 2, 1>(A, CS.c[2], j0, j1, r, x, xc, rc); break;
+      case 5: gs_lines<false, false, false, 1, 1>(A, CS.c[1], j0, j1, r, x, xc, rc); break;
+      default: gs_lines<false, false, RES, 0, 1>(A, CS.c[0], j0, j1, r, x, xc, rc); break;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) red_release_gpu(W.ctr + s * W.nzq + jz, 1);
+  }
+  // the last block to leave resets the counters for the next launch
+  __shared__ int last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket + 1, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    for (int i = threadIdx.x; i < 7 * W.nzq; i += blockDim.x) W.ctr[i] = 0;
+    if (threadIdx.x == 0) {
+      ticket[0] = 0;
+      ticket[1] = 0;
+      ticket[2] = 0;
+    }
+  }
 }
 
 // Residual restricted at the injected points (colour 0: even ix, iy, iz):
@@ -1439,6 +1616,114 @@ template int launch_prolong<double>(const LevelDev &, int64_t, const double *, d
                                     const int *, cudaStream_t);
 template int launch_prolong<float>(const LevelDev &, int64_t, const float *, float *, const int *,
                                    cudaStream_t);
+
+std::vector<int2> wave_plan(LevelDev &L, int lag, int rows_per_item) {
+  std::vector<int2> tab;
+  L.wave_ntab = L.wave_total = L.wave_lpi = L.wave_nzq = 0;
+  for (int q = 0; q < 4; ++q) L.wave_ipp[q] = 0;
+  const int nzq = (L.nz + 1) / 2;
+  // every class needs lines on its planes (ny, nz >= 2) for the waits on the
+  // previous stage alone to order all earlier ones
+  if (L.nx < 1 || L.ny < 2 || L.nz < 2 || nzq >= (1 << 15) || lag < 2) return tab;
+  int maxnyq = 1;
+  for (int q = 0; q < 4; ++q) maxnyq = std::max(maxnyq, L.cls[q].nyq);
+  const int lpi = std::min(maxnyq, std::max(1, rows_per_item / L.nx));
+  int ipp[4];
+  for (int q = 0; q < 4; ++q) ipp[q] = (L.cls[q].nyq + lpi - 1) / lpi;
+  struct Entry { int key, s, jz; };
+  std::vector<Entry> es;
+  for (int s = 0; s < 7; ++s) {
+    const int q = wave_class(s), pz = q >> 1;
+    if (ipp[q] == 0) continue;
+    for (int jz = 0; pz + 2 * jz < L.nz; ++jz) es.push_back({pz + 2 * jz + lag * s, s, jz});
+  }
+  std::sort(es.begin(), es.end(), [](const Entry &a, const Entry &b) {
+    return a.key != b.key ? a.key < b.key : a.s < b.s;
+  });
+  int64_t total = 0;
+  for (const Entry &e : es) {
+    tab.push_back(make_int2((e.s << 16) | e.jz, (int)total));
+    total += ipp[wave_class(e.s)];
+  }
+  if (tab.empty() || total >= INT_MAX / 2) return std::vector<int2>();
+  L.wave_ntab = (int)tab.size();
+  L.wave_total = (int)total;
+  L.wave_lpi = lpi;
+  L.wave_nzq = nzq;
+  for (int q = 0; q < 4; ++q) L.wave_ipp[q] = ipp[q];
+  return tab;
+}
+
+template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
+void wave_go(const LevelDev &L, const LevelMat<VT> &A, const WaveDev &W, const RT *r, T *x,
+             const T *xc, T *rc, const int *done, cudaStream_t s) {
+  // persistent grid: as many blocks as fit on the GPU at once (the waits do
+  // not depend on it), never more than there are items
+  const size_t smem = (W.uniform > 0 && W.ntab <= kWaveSmemEntries) ? W.ntab * sizeof(int) : 0;
+  static int sms = 0, per_sm[kWaveSmemEntries / 256 + 1] = {};
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    sms = std::max(1, sms);
+  }
+  int &ps = per_sm[(smem / sizeof(int) + 255) / 256];   // by table size in 1 KB steps
+  if (!ps) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_gs_wave<ZERO, PRO, RES, VT, T, RT>,
+                                                  kThreads, (smem / 1024 + 1) * 1024);
+    ps = std::max(1, ps);
+  }
+  const int grid = std::min(sms * ps, W.total);
+  k_gs_wave<ZERO, PRO, RES><<<grid, kThreads, smem, s>>>(A, classes_of(L), W, r, x, xc, rc, done);
+}
+
+template <class T, class RT>
+int launch_gs_wave(const LevelDev &L, int mode, const RT *r, T *x, const T *xc, T *rc,
+                   const int *done, cudaStream_t s) {
+  using VT = typename ValsOf<T>::VT;
+  if (!L.wave_tab || !L.wave_ctr || L.wave_total == 0) return 0;
+  const LevelMat<VT> A = mat_of(L, ValsOf<T>::get(L));
+  WaveDev W;
+  W.tab = L.wave_tab;
+  W.ctr = L.wave_ctr;
+  W.ntab = L.wave_ntab;
+  W.total = L.wave_total;
+  W.lpi = L.wave_lpi;
+  W.nzq = L.wave_nzq;
+  W.nz = L.nz;
+  for (int q = 0; q < 4; ++q) W.ipp[q] = L.wave_ipp[q];
+  W.uniform = L.wave_ipp[0];
+  for (int q = 1; q < 4; ++q)
+    if (L.wave_ipp[q] != W.uniform) W.uniform = 0;
+  switch (mode) {
+    case GS_PLAIN: wave_go<false, false, false>(L, A, W, r, x, xc, rc, done, s); break;
+    case GS_ZERO_GUESS: wave_go<true, false, false>(L, A, W, r, x, xc, rc, done, s); break;
+    case GS_ZERO_GUESS | GS_RESTRICT:
+      wave_go<true, false, true>(L, A, W, r, x, xc, rc, done, s);
+      break;
+    case GS_PROLONG: wave_go<false, true, false>(L, A, W, r, x, xc, rc, done, s); break;
+    default: return 0;
+  }
+  return 1;
+}
+template int launch_gs_wave<double, double>(const LevelDev &, int, const double *, double *,
+                                            const double *, double *, const int *, cudaStream_t);
+template int launch_gs_wave<float, double>(const LevelDev &, int, const double *, float *,
+                                           const float *, float *, const int *, cudaStream_t);
+template int launch_gs_wave<float, float>(const LevelDev &, int, const float *, float *,
+                                          const float *, float *, const int *, cudaStream_t);
+
+int read_wave_fault(unsigned int *fault) {
+  *fault = 0u;
+  cudaError_t e = cudaMemcpyFromSymbol(fault, g_wave_fault, sizeof(*fault));
+  if (e != cudaSuccess) return (int)e;
+  if (*fault) {
+    const unsigned int zero = 0u;
+    e = cudaMemcpyToSymbol(g_wave_fault, &zero, sizeof(zero));
+    if (e != cudaSuccess) return (int)e;
+  }
+  return 0;
+}
 
 int read_check_record(unsigned long long *record) {
   *record = 0ull;

@@ -2,6 +2,8 @@
 #pragma once
 #include "common.cuh"
 
+#include <vector>
+
 namespace hpcgx {
 
 // One multigrid level on the device.
@@ -24,6 +26,11 @@ struct LevelDev {
   // correction; level 0 uses the caller's vectors)
   double *r64 = nullptr, *x64 = nullptr;
   float *r32 = nullptr, *x32 = nullptr;
+  // one-launch symmetric sweep (k_gs_wave): ticket table and counters
+  int2 *wave_tab = nullptr;   // wave_ntab entries
+  int *wave_ctr = nullptr;    // 7 * wave_nzq + 3 ints, zero between launches
+  int wave_ntab = 0, wave_total = 0, wave_lpi = 0, wave_nzq = 0;
+  int wave_ipp[4] = {};
 };
 
 // Device-side state of a CG solve (scalars never leave the GPU except the
@@ -133,6 +140,18 @@ int launch_restrict_residual(const LevelDev &F, int64_t nc, const RT *rf, const 
 template <class T>
 int launch_prolong(const LevelDev &F, int64_t nc, const T *xc, T *xf, const int *done,
                    cudaStream_t s);
+// One symmetric Gauss-Seidel sweep of a level in one launch (k_gs_wave), the
+// same result as its seven class launches.  mode: GS_PLAIN, or GS_ZERO_GUESS
+// (optionally | GS_RESTRICT into rc), or GS_PROLONG (adding xc first).
+// wave_plan fills the wave_* fields of L but the two device pointers and
+// returns the ticket table to upload (items of about rows_per_item rows,
+// stage lag `lag` planes); an empty table disables the launch.
+std::vector<int2> wave_plan(LevelDev &L, int lag, int rows_per_item);
+template <class T, class RT>
+int launch_gs_wave(const LevelDev &L, int mode, const RT *r, T *x, const T *xc, T *rc,
+                   const int *done, cudaStream_t s);
+// 1 if a one-launch sweep gave up waiting since the last call (then cleared)
+int read_wave_fault(unsigned int *fault);
 template <class ZT>
 int launch_cg_rz(int64_t n, const double *r, const ZT *z, const double *Ap, const Reduce &red,
                   CgState *st, cudaStream_t s);

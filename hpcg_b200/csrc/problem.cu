@@ -120,6 +120,11 @@ namespace hpcgx {
 int set_error(int code, const char *msg) { return fail(code, msg); }
 }  // namespace hpcgx
 
+static int env_int(const char *name, int dflt) {
+  const char *e = std::getenv(name);
+  return e && *e ? std::atoi(e) : dflt;
+}
+
 struct hpcgx_problem {
   int device = 0;
   int nlev = 0;
@@ -167,6 +172,18 @@ struct hpcgx_problem {
   double *gsum = nullptr;            // this rank's deferred reduction totals
   double *hstage[kMaxLevels] = {};   // haloed FP64 staging of operator inputs
   bool sharded() const { return nranks > 1 || nccl != nullptr || comm_halo != nullptr; }
+  // symmetric sweeps in one launch (k_gs_wave) instead of seven class launches
+  bool wave = false;
+  bool use_wave(int l) const { return wave && L[l].wave_tab != nullptr; }
+  // a one-launch sweep that gave up waiting is reported once the stream is idle
+  int wave_check() {
+    if (!wave) return HPCGX_OK;
+    unsigned int f = 0u;
+    const int e = read_wave_fault(&f);
+    if (e != 0) return cuda_fail((cudaError_t)e);
+    if (f) return fail(HPCGX_ETIMEOUT, "a one-launch Gauss-Seidel sweep gave up waiting for a stage");
+    return HPCGX_OK;
+  }
 
   ~hpcgx_problem();
   int alloc(void **ptr, size_t n) {
@@ -265,6 +282,29 @@ struct hpcgx_problem {
     });
   }
 
+  // One symmetric sweep of level l in one launch; probed as the finest
+  // level's Gauss-Seidel with the bytes of its seven class steps.
+  template <class T, class RT0>
+  int wave_launch(int l, int mode, const void *r, T *x, const T *xc, T *rc, const int *done) {
+    const bool mixed = std::is_same<T, float>::value;
+    const int kinds = l == 0 ? HPCGX_PROBE_GS_FINE : 0;
+    double bytes = 0.0;
+    if (kinds & probe) {
+      const int m0 = mode & GS_ZERO_GUESS;
+      for (int q = 0; q < 3; ++q)
+        bytes += gs_bytes(l, q, (q == 0 && (mode & GS_PROLONG)) ? GS_PROLONG : m0, mixed);
+      bytes += gs_bytes(l, 3, GS_SYM3 | m0, mixed);
+      for (int q = 2; q >= 0; --q)
+        bytes += gs_bytes(l, q, (q == 0 && (mode & GS_RESTRICT)) ? GS_RESTRICT : GS_PLAIN, mixed);
+    }
+    return probed(kinds, bytes, [&]() {
+      if (l == 0)
+        return launch_gs_wave<T, RT0>(L[l], mode, static_cast<const RT0 *>(r), x, xc, rc, done,
+                                      stream);
+      return launch_gs_wave<T, T>(L[l], mode, static_cast<const T *>(r), x, xc, rc, done, stream);
+    });
+  }
+
   // One V-cycle (src/ComputeMG_ref.cpp:39-63) with all levels fused as
   // described in kernels.cu.  r0 / x0 are the finest level's vectors.
   template <class T, class RT0>
@@ -276,9 +316,15 @@ struct hpcgx_problem {
       xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
     }
     // Each symmetric sweep: forward classes 0..2, class 3 forward+backward in
-    // one launch (GS_SYM3), backward classes 2..0 -- 7 launches.
+    // one launch (GS_SYM3), backward classes 2..0 -- 7 launches, or one
+    // k_gs_wave launch doing the same seven steps.
     // descend: pre-smooth (zero initial guess) and restrict
     for (int l = 0; l + 1 < nlev; ++l) {
+      if (use_wave(l)) {
+        TRY((wave_launch<T, RT0>(l, GS_ZERO_GUESS | GS_RESTRICT, rl[l], xl[l], nullptr,
+                                 lvl_r(L[l + 1], (T *)nullptr), done)));
+        continue;
+      }
       for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr, done)));
       TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr,
@@ -289,14 +335,23 @@ struct hpcgx_problem {
     }
     // coarsest level: one symmetric sweep from zero
     const int c = nlev - 1;
-    for (int q = 0; q < 3; ++q)
-      TRY((gs_launch<T, RT0>(c, q, 0, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
-    TRY((gs_launch<T, RT0>(c, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr,
-                           done)));
-    for (int q = 2; q >= 0; --q)
-      TRY((gs_launch<T, RT0>(c, q, 1, GS_PLAIN, rl[c], xl[c], nullptr, nullptr, done)));
+    if (use_wave(c)) {
+      TRY((wave_launch<T, RT0>(c, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
+    } else {
+      for (int q = 0; q < 3; ++q)
+        TRY((gs_launch<T, RT0>(c, q, 0, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
+      TRY((gs_launch<T, RT0>(c, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr,
+                             done)));
+      for (int q = 2; q >= 0; --q)
+        TRY((gs_launch<T, RT0>(c, q, 1, GS_PLAIN, rl[c], xl[c], nullptr, nullptr, done)));
+    }
     // ascend: prolongate and post-smooth
     for (int l = nlev - 2; l >= 0; --l) {
+      if (use_wave(l)) {
+        TRY((wave_launch<T, RT0>(l, GS_PROLONG, rl[l], xl[l], lvl_x(L[l + 1], (T *)nullptr),
+                                 nullptr, done)));
+        continue;
+      }
       for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, q == 0 ? GS_PROLONG : GS_PLAIN, rl[l], xl[l],
                                lvl_x(L[l + 1], (T *)nullptr), nullptr, done)));
@@ -309,6 +364,10 @@ struct hpcgx_problem {
 
   template <class T, class RT>
   int symgs(int l, const RT *r, T *x) {
+    if (use_wave(l)) {
+      note(launch_gs_wave<T, RT>(L[l], GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
+      return HPCGX_OK;
+    }
     for (int q = 0; q < 3; ++q)
       note(launch_gs_class<T, RT>(L[l], q, 0, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
     note(launch_gs_class<T, RT>(L[l], 3, 0, GS_SYM3, r, x, nullptr, nullptr, nullptr, stream));
@@ -498,6 +557,7 @@ struct hpcgx_problem {
     }
     if (xu != x) CK(cudaMemcpyAsync(xu, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     CK(cudaStreamSynchronize(stream));
+    TRY(wave_check());
     if (niters) *niters = h.niters;
     if (normr) *normr = h.normr;
     if (normr0) *normr0 = h.normr0;
@@ -560,6 +620,14 @@ struct hpcgx_problem {
   void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done,
                    const T *xc = nullptr, T *rc = nullptr) {
     const int m0 = zero ? GS_ZERO_GUESS : GS_PLAIN;
+    if (use_wave(l)) {
+      const int m = xc ? GS_PROLONG : m0 | (rc ? GS_RESTRICT : 0);
+      add(pl, [=]() {
+        note(launch_gs_wave<T, RT>(L[l], m, r, x, xc, rc, done, stream));
+        return HPCGX_OK;
+      });
+      return;
+    }
     for (int q = 0; q < 3; ++q) {
       const int m = (q == 0 && xc) ? GS_PROLONG : m0;
       add(pl, [=]() {
@@ -1170,6 +1238,7 @@ int sharded_cg(const std::vector<hpcgx_problem *> &ps, const Runner &run, int ki
     CK(cudaMemcpyAsync(x[r], ps[r]->x, ps[r]->L[0].n * sizeof(double), cudaMemcpyDeviceToDevice,
                        ps[r]->stream));
   for (hpcgx_problem *p : ps) TRY(bounded_wait(p->stream));
+  for (hpcgx_problem *p : ps) TRY(p->wave_check());
   if (niters) *niters = h.niters;
   if (normr) *normr = h.normr;
   if (normr0) *normr0 = h.normr0;
@@ -1184,6 +1253,7 @@ int sharded_op(const std::vector<hpcgx_problem *> &ps, const Runner &run, BUILD 
   for (size_t r = 0; r < ps.size(); ++r) TRY(build(ps[r], plans[r], (int)r));
   TRY(run(plans));
   for (hpcgx_problem *p : ps) TRY(bounded_wait(p->stream));
+  for (hpcgx_problem *p : ps) TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1234,6 +1304,13 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   hpcgx_problem *p = new hpcgx_problem;
   p->device = device;
   p->nlev = levels;
+  // sweep form: the seven class launches, or with HPCGX_GS_WAVE=1 the
+  // one-launch sweep (bit-identical; slower on B200 at 512^3: 3.79 ms per
+  // finest-level sweep against 3.32 ms), whose stage lag (planes) and item
+  // size (rows) can be tuned
+  p->wave = env_int("HPCGX_GS_WAVE", 0) != 0;
+  const int wave_lag = env_int("HPCGX_WAVE_LAG", 6);
+  const int wave_rows = env_int("HPCGX_WAVE_ROWS", 2048);
   p->nranks = nranks;
   p->rank = rank;
   int rc = HPCGX_OK;
@@ -1250,6 +1327,17 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
     plan_level(A, nx >> l, ny >> l, nz >> l);
     A.zlo = rank > 0;
     A.zhi = rank + 1 < nranks;
+    {
+      const std::vector<int2> tab = wave_plan(A, wave_lag, wave_rows);
+      if (!tab.empty()) {
+        const size_t nctr = (size_t)7 * A.wave_nzq + 3;
+        if ((rc = p->alloc((void **)&A.wave_tab, tab.size() * sizeof(int2)))) return bail(rc);
+        if ((rc = p->alloc((void **)&A.wave_ctr, nctr * sizeof(int)))) return bail(rc);
+        e = cudaMemcpy(A.wave_tab, tab.data(), tab.size() * sizeof(int2), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(A.wave_ctr, 0, nctr * sizeof(int));
+        if (e != cudaSuccess) return bail(cuda_fail(e));
+      }
+    }
     const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
     if ((rc = p->alloc((void **)&A.vals, slots * sizeof(double)))) return bail(rc);
     if ((rc = p->alloc((void **)&A.cols, slots * sizeof(int32_t)))) return bail(rc);
@@ -1461,6 +1549,7 @@ int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
   }
   TRY((p->symgs<double, double>(level, r, x)));
   CK(cudaStreamSynchronize(p->stream));
+  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1477,6 +1566,7 @@ int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
   }
   TRY((p->vcycle<double, double>(r, x, nullptr)));
   CK(cudaStreamSynchronize(p->stream));
+  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1506,6 +1596,7 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
   else
     TRY((p->symgs<float, float>(level, r32, x)));
   CK(cudaStreamSynchronize(p->stream));
+  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1517,6 +1608,7 @@ int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x) {
   TRY(p->check_ready(true));
   TRY((p->vcycle<float, double>(r, x, nullptr)));
   CK(cudaStreamSynchronize(p->stream));
+  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1746,6 +1838,10 @@ int hpcgx_synchronize(hpcgx_problem *p) {
 
 int hpcgx_check_status(void) {
   CK(cudaDeviceSynchronize());
+  unsigned int wf = 0u;
+  const int we = read_wave_fault(&wf);
+  if (we != 0) return cuda_fail((cudaError_t)we);
+  if (wf) return fail(HPCGX_ETIMEOUT, "a one-launch Gauss-Seidel sweep gave up waiting for a stage");
   unsigned long long rec = 0ull;
   const int e = read_check_record(&rec);
   if (e != 0) return cuda_fail((cudaError_t)e);
