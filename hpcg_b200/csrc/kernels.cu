@@ -746,14 +746,14 @@ k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, 
 // stops the launch's remaining items.  The last block to leave resets the
 // counters for the next launch.
 //
-// What it is for: each class launch reads the x-neighbourhood of its rows in
-// all z-planes, i.e. the whole x vector, from DRAM; the wavefront keeps the
-// few planes between its first and last stage in L2, so x and the right-hand
-// side pass through DRAM about once per sweep instead of once per step.
-// Measured on B200 at 512^3 (mixed V-cycle, finest level) it is slower than
-// the class launches all the same -- 3.79 ms per symmetric sweep at lag 6 and
-// 2048-row items against 3.32 ms, the lag hardly mattering -- so it is an
-// option (HPCGX_GS_WAVE=1), not the default.
+// What it was for: each class launch reads the x-neighbourhood of its rows in
+// all z-planes, i.e. the whole x vector, from DRAM; a wavefront could keep the
+// planes between a plane's first and last stage in L2.  Measured on B200 at
+// 512^3 (mixed V-cycle, finest level) the matrix values streaming past in
+// between (~0.9 GB) evict them -- DRAM traffic per sweep is no lower than the
+// class launches' -- and the per-item serial steps lower the DRAM rate:
+// 3.79 ms per symmetric sweep at lag 6 and 2048-row items against 3.32 ms.
+// So it is an option (HPCGX_GS_WAVE=1), not the default.
 
 struct WaveDev {
   const int2 *tab;   // (stage << 16 | class plane, first ticket), ticket order
