@@ -79,6 +79,7 @@ SIGNATURES = {
     "hpcgx_attach_nccl": (_I, [_P, _P, _I]),
     "hpcgx_attach_comm": (_I, [_P, HALO_FN, SUM_FN, _P]),
     "hpcgx_check_status": (_I, []),
+    "hpcgx_wave_schedule": (_I, [_I, _I, _I, _I, _I, _I, _IP, _IP, _IP, _IP, _IP, _IP]),
     "hpcgx_group_create": (_I, [_P, _I, C.POINTER(_P)]),
     "hpcgx_group_destroy": (_I, [_P]),
     "hpcgx_group_spmv": (_I, [_P, _I, _P, _P]),

@@ -1855,6 +1855,29 @@ int hpcgx_check_status(void) {
                                 " index " + std::to_string(index) + " out of range");
 }
 
+int hpcgx_wave_schedule(int nx, int ny, int nz, int lag, int rows_per_item, int cap, int *codes,
+                        int *starts, int *count, int *total, int *lines_per_item,
+                        int *items_per_plane) {
+  if (nx < 1 || ny < 1 || nz < 1 || cap < 0 || !count || !total || !lines_per_item ||
+      !items_per_plane || (cap > 0 && (!codes || !starts)))
+    return fail(HPCGX_EINVAL, "bad arguments");
+  if ((int64_t)nx * ny * (nz + 2) >= (int64_t)1 << 31)
+    return fail(HPCGX_EINVAL, "more than 2^31 rows");
+  LevelDev L;
+  plan_level(L, nx, ny, nz);
+  const std::vector<int2> tab = wave_plan(L, lag, rows_per_item);
+  *count = (int)tab.size();
+  *total = L.wave_total;
+  *lines_per_item = L.wave_lpi;
+  for (int q = 0; q < 4; ++q) items_per_plane[q] = L.wave_ipp[q];
+  if ((int)tab.size() > cap) return fail(HPCGX_EINVAL, "table larger than cap");
+  for (size_t i = 0; i < tab.size(); ++i) {
+    codes[i] = tab[i].x;
+    starts[i] = tab[i].y;
+  }
+  return HPCGX_OK;
+}
+
 // ---- sharding
 int hpcgx_nccl_unique_id(void *id, int bytes) {
   if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");

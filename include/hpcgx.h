@@ -227,6 +227,17 @@ int hpcgx_synchronize(hpcgx_problem *p);
  * access itself was redirected into the buffers), else HPCGX_OK.  Synchronises
  * the device.  Always HPCGX_OK in the regular build, which has no checks. */
 int hpcgx_check_status(void);
+/* Diagnostics, host only (no device needed): the ticket table of the
+ * one-launch symmetric sweep (k_gs_wave, HPCGX_GS_WAVE=1) of an nx x ny x nz
+ * level with the given stage lag (planes) and item size (rows).  Entry i is
+ * stage codes[i] >> 16 (0..6: forward classes 0-2, class 3 both ways,
+ * backward classes 2-0) on class plane codes[i] & 0xffff, with tickets
+ * starts[i] .. starts[i] + items_per_plane[class] - 1.  *count = 0 where the
+ * sweep is not available (ny or nz below 2, lag below 2); HPCGX_EINVAL if
+ * more than cap entries would be written (*count holds the number needed). */
+int hpcgx_wave_schedule(int nx, int ny, int nz, int lag, int rows_per_item, int cap, int *codes,
+                        int *starts, int *count, int *total, int *lines_per_item,
+                        int *items_per_plane);
 
 /* ---- sharding over ranks (z-slabs) --------------------------------------
  * The reference's MPI decomposition with a process grid of 1 x 1 x nranks
