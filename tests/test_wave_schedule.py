@@ -9,7 +9,10 @@ device is needed.  The sweep's bounded waits rely on these properties:
     (s, z), so a block only ever waits for tickets already taken by running
     blocks (the waits end whatever the number of co-resident blocks);
   * the sweep is unavailable (empty table) where a class has no line next to
-    some plane (ny or nz below 2) or the lag is below 2.
+    some plane (ny or nz below 2) or the lag is below 2;
+  * those waits suffice: the table's items, run one at a time in random orders
+    that only respect the waits, reproduce the oracle's colour-ordered SYMGS
+    bit for bit (and a weaker wait does not).
 """
 import ctypes as C
 
@@ -96,3 +99,103 @@ def test_bad_arguments_are_rejected():
                                  C.byref(lpi), ipp) == 1
     assert h.hpcgx_wave_schedule(4, 4, 4, 4, 64, 8, None, None, C.byref(count), C.byref(total),
                                  C.byref(lpi), ipp) == 1
+
+
+# ---------------------------------------------------------------------------
+# Execution model: the items of the library's table run one at a time in a
+# random order that only respects the sweep's waits.  Every such order must
+# reproduce the oracle's colour-ordered SYMGS bit for bit; an order allowed by
+# a weaker wait (stage s-1 on plane z only) must not.
+
+def _gs_rows(lev, rows, r, x):
+    """Reference GS update of independent rows (src/ComputeSYMGS_ref.cpp:67-81),
+    vectorised; the slot order of each row is kept."""
+    import numpy as np
+    if rows.size == 0:
+        return
+    nnz = lev.nnz[rows].astype(np.int64)
+    cols = lev.cols.reshape(-1, 27)[rows]
+    vals = lev.vals.reshape(-1, 27)[rows]
+    d = vals[np.arange(rows.size), lev.diag[rows]]
+    s = r[rows].copy()
+    for j in range(27):
+        m = j < nnz
+        s[m] = s[m] - vals[m, j] * x[cols[m, j]]
+    s = s + x[rows] * d
+    x[rows] = s / d
+
+
+def _item_rows(nx, ny, q, jz, b, lpi, px):
+    import numpy as np
+    py, pz = q & 1, q >> 1
+    nyq = (ny - py + 1) // 2
+    j0 = jz * nyq + b * lpi
+    j1 = min(j0 + lpi, (jz + 1) * nyq)
+    iz = pz + 2 * jz
+    out = []
+    for j in range(j0, j1):
+        iy = py + 2 * (j - jz * nyq)
+        ix = np.arange(px, nx, 2)
+        out.append((iz * ny + iy) * nx + ix)
+    return np.concatenate(out) if out else np.zeros(0, np.int64)
+
+
+def _run_item(lev, nx, ny, s, jz, b, lpi, r, x):
+    q = stage_class(s)
+    if s < 3:
+        phases = [(q, 0), (q, 1)]
+    elif s == 3:
+        phases = [(3, 0), (3, 1), (3, 1), (3, 0)]   # 6 fwd, 7 fwd, 7 bwd, 6 bwd
+    else:
+        phases = [(q, 1), (q, 0)]
+    for qq, px in phases:
+        _gs_rows(lev, _item_rows(nx, ny, qq, jz, b, lpi, px), r, x)
+
+
+def _random_order_sweep(lev, dims, tab, ipp, lpi, r, x, rng, weak=False):
+    nx, ny, nz = dims
+    items = [(s, jz, b) for s, jz, _ in tab for b in range(ipp[stage_class(s)])]
+    done = {}
+    pending = list(items)
+    while pending:
+        ready = []
+        for k, (s, jz, b) in enumerate(pending):
+            if s == 0:
+                ready.append(k)
+                continue
+            z = (stage_class(s) >> 1) + 2 * jz
+            qp = stage_class(s - 1)
+            planes = (z,) if weak else (z - 1, z, z + 1)
+            ok = all(done.get((s - 1, (zz - (qp >> 1)) // 2), 0) == ipp[qp]
+                     for zz in planes if 0 <= zz < nz and (zz & 1) == (qp >> 1))
+            if ok:
+                ready.append(k)
+        assert ready, "no item can run: the waits deadlock"
+        k = ready[rng.integers(len(ready))]
+        s, jz, b = pending.pop(k)
+        _run_item(lev, nx, ny, s, jz, b, lpi, r, x)
+        done[(s, jz)] = done.get((s, jz), 0) + 1
+    return x
+
+
+@pytest.mark.parametrize("dims,lag,rows", [((8, 8, 8), 2, 1), ((6, 4, 6), 3, 1),
+                                           ((5, 6, 7), 2, 1), ((8, 6, 10), 4, 16)])
+def test_any_order_the_waits_allow_reproduces_the_colour_sweep(dims, lag, rows, oracle):
+    import numpy as np
+    L, _, _, _ = oracle.hierarchy(*dims, levels=1)
+    oracle.colour_order(L)
+    lev = L[0]
+    r = oracle.uniform(12, lev.nrow)
+    x0 = oracle.uniform(13, lev.nrow)
+    want = oracle.symgs(lev, r, x0, coloured=True)
+    tab, total, lpi, ipp = schedule(*dims, lag, rows)
+    rng = np.random.default_rng(7)
+    for _ in range(6):
+        got = _random_order_sweep(lev, dims, tab, ipp, lpi, r, x0.copy(), rng)
+        assert (got == want).all()
+    # control: waiting for the previous stage on plane z alone is not enough
+    wrong = 0
+    for _ in range(6):
+        got = _random_order_sweep(lev, dims, tab, ipp, lpi, r, x0.copy(), rng, weak=True)
+        wrong += not (got == want).all()
+    assert wrong > 0
