@@ -10,7 +10,10 @@ with an all-reduce (src/ComputeDotProduct_ref.cpp:66-77).  The results must
 equal, bit for bit, the oracle's global restatement of the same algorithm
 (Oracle.slab_hierarchy: block-Jacobi SYMGS with the other slabs' values
 frozen at the start of each sweep, per-slab dot products summed in rank
-order), which the GPU group is tested against.
+order), which the GPU group is tested against.  The library's order of the
+V-cycle on a slab (restriction and prolongation fused into the sweeps, two
+one-plane fix-ups around the exchanges) is restated too and must give the
+reference order's result.
 """
 import ctypes as C
 import os
@@ -133,6 +136,45 @@ def _worker(rank, world, port, out):
         e[s.plane:s.plane + s.S] = xf
         symgs(s, r, e)
 
+    def mg_fused(l, r, e, fix=True):
+        """The library's order of the same V-cycle on a slab: the residual at
+        the injected points is formed inside the pre-smoother with the halo
+        the sweep read, then the halo is exchanged and only the first plane's
+        injected residuals (the one plane that reads the halo below; the local
+        z-extent is even) are formed again; the correction of the first plane
+        is added before the exchange that precedes the post-smoother, the
+        rest after it.  fix=False leaves the two fix-ups out (a planted
+        mistake: the result must then differ)."""
+        s = slabs[l]
+        e[:] = 0.0                      # the first sweep's halo: zero, not exchanged
+        lib.or_symgs(C.c_int64(s.S), _p(s.nnz), _p(s.cols), _p(s.vals), _p(s.diag),
+                     _p(s.order), _p(r), _p(e, s.plane))
+        if s.f2c is None:
+            return
+        nc = s.f2c.size
+        Axf = np.zeros(s.S)
+        lib.or_spmv(C.c_int64(s.S), _p(s.nnz), _p(s.cols), _p(s.vals), _p(e, s.plane), _p(Axf))
+        rc = np.zeros(nc)
+        lib.or_restriction(C.c_int64(nc), _p(s.f2c), _p(r), _p(Axf), _p(rc))
+        exchange(s, e)
+        first = s.f2c < s.plane          # injected points of the first plane
+        assert (s.f2c[~first] >= s.plane).all()
+        if rank > 0 and fix:
+            lib.or_spmv(C.c_int64(s.S), _p(s.nnz), _p(s.cols), _p(s.vals), _p(e, s.plane),
+                        _p(Axf))
+            rc[first] = r[s.f2c[first]] - Axf[s.f2c[first]]
+        ec = slabs[l + 1].ext()
+        mg_fused(l + 1, rc, ec, fix)
+        xc = ec[slabs[l + 1].plane:slabs[l + 1].plane + nc]
+        xf = e[s.plane:s.plane + s.S]
+        if rank > 0 and fix:
+            xf[s.f2c[first]] = xf[s.f2c[first]] + xc[first]
+        exchange(s, e)
+        rest = ~first if rank > 0 and fix else np.ones(nc, bool)
+        xf[s.f2c[rest]] = xf[s.f2c[rest]] + xc[rest]
+        lib.or_symgs(C.c_int64(s.S), _p(s.nnz), _p(s.cols), _p(s.vals), _p(s.diag),
+                     _p(s.order), _p(r), _p(e, s.plane))
+
     def dot(x, y):
         local = torch.tensor([lib.or_dot(C.c_int64(x.size), _p(x), _p(y))], dtype=torch.float64)
         dist.all_reduce(local)
@@ -162,6 +204,12 @@ def _worker(rank, world, port, out):
     e = s0.ext()
     mg(0, np.ascontiguousarray(rr[lo:hi]), e)
     res["mg"] = e[s0.plane:s0.plane + s0.S].copy()
+    e = s0.ext()
+    mg_fused(0, np.ascontiguousarray(rr[lo:hi]), e)
+    res["mg_fused"] = e[s0.plane:s0.plane + s0.S].copy()
+    e = s0.ext()
+    mg_fused(0, np.ascontiguousarray(rr[lo:hi]), e, fix=False)
+    res["mg_nofix"] = e[s0.plane:s0.plane + s0.S].copy()
     # CG_ref (src/CG_ref.cpp:58-144), 12 iterations, with exchanges and all-reduces
     b = np.zeros(s0.S)
     spmv(s0, s0.ext(u[lo:hi]), b)
@@ -212,6 +260,8 @@ def test_slab_oracle_matches_per_rank_exchange_two_gloo_ranks(oracle):
     assert (cat("spmv") == oracle.spmv(L[0], u)).all()
     assert (cat("symgs") == oracle.symgs(L[0], rr, x0, coloured=True)).all()
     assert (cat("mg") == oracle.mg(L, rr, coloured=True)).all()
+    assert (cat("mg_fused") == cat("mg")).all()
+    assert not (cat("mg_nofix") == cat("mg")).all()
     b = oracle.spmv(L[0], u)
     xs, k, nr, nr0 = oracle.cg(L, b, np.zeros(n), 12, 0.0, precond=True, coloured=True)
     assert k == 12
