@@ -16,8 +16,11 @@ it for the mixed-vs-FP64 comparison.  Inputs are generated on the device
                bytes / CUDA-event duration of every launch in the timed region,
                against the measured HBM copy bandwidth
   cpu_baseline the reference's own CG_ref (oracle/_ref, OpenMP on all host
-               cores) per-iteration time on a 128^3 sample, scaled to 512^3
-               rows and to the FP64 solve's iteration count
+               cores): the per-iteration time of a few iterations on a 256^3
+               sample of the same problem (b = A u), scaled x8 in rows to
+               512^3 and to the reference's own (natural-order) iteration
+               count to 1e-10, measured at 32^3 - 256^3 and extrapolated to
+               512^3 (the reference's int32 counters overflow there)
 
 Multi-GPU (torchrun, N ranks): one system of N z-slabs, each GPU holding one
 512^3 slab (weak scaling; the reference's 1 x 1 x N process grid): halo planes
@@ -157,9 +160,35 @@ def max_over_ranks(values, dist=None, device=None):
     return t.tolist()
 
 
-def cpu_reference_sample(iters_512, dims, sample_n=128, sample_it=10):
-    """CG_ref of the reference build (oracle/_ref) on a sample_n^3 problem:
-    per-iteration time of a bounded run, scaled to dims rows and iters_512."""
+# The reference's own CG_ref (natural row order, src/CG_ref.cpp with
+# src/ComputeSYMGS_ref.cpp) on the bench's system b = A u, u ~ U(-1, 1) seed 1,
+# x0 = 0: iterations to ||r||/||r0|| <= 1e-10, measured with oracle/_ref
+# (the reference compiled from its sources) on cubic grids.
+REF_NATURAL_ITERS = {32: 24, 64: 40, 128: 71, 256: 128}
+
+
+def reference_iterations(n):
+    """CG_ref's iteration count to 1e-10 on the n^3 bench system: measured up
+    to 256^3; beyond, each doubling of the grid multiplies the count by the
+    ratio of the last measured doubling (geometric extrapolation)."""
+    known = {k: v for k, v in REF_NATURAL_ITERS.items() if v > 0}
+    if n in known:
+        return known[n], "measured"
+    top = max(known)
+    prev = top // 2
+    it, size = float(known[top]), top
+    ratio = known[top] / float(known[prev])
+    while size < n:
+        it *= ratio
+        size *= 2
+    return int(round(it)), ("extrapolated from %d (%d^3) and %d (%d^3): x%.3f per doubling"
+                            % (known[prev], prev, known[top], top, ratio))
+
+
+def cpu_reference_sample(dims, sample_n=256, sample_it=3):
+    """CG_ref of the reference build (oracle/_ref) on a sample_n^3 problem of
+    the same kind (b = A u): the per-iteration time of a bounded run, scaled
+    to dims rows and to CG_ref's own iteration count on dims."""
     from oracle.oracle import RefProblem, Oracle
     if not RefProblem.available():
         return None
@@ -175,13 +204,17 @@ def cpu_reference_sample(iters_512, dims, sample_n=128, sample_it=10):
     ref.close()
     per_it = dt / k
     scale = (dims[0] * dims[1] * dims[2]) / float(n)
-    value = per_it * scale * iters_512
+    iters, basis = reference_iterations(dims[0]) if dims[0] == dims[1] == dims[2] else (0, "")
+    value = per_it * scale * iters
     return {"value": value, "unit": "s", "cores": int(os.environ.get("OMP_NUM_THREADS", threads)),
             "kind": "reference",
             "sample": "reference CG_ref (oracle/_ref, -O3 OpenMP, serial SYMGS as in "
-                      "src/ComputeSYMGS_ref.cpp) on %d^3, %d iterations in %.2f s = %.3f s/iter; "
-                      "scaled x%.0f rows to %dx%dx%d and x%d iterations (the FP64 solve's count)"
-                      % (sample_n, k, dt, per_it, scale, dims[0], dims[1], dims[2], iters_512)}
+                      "src/ComputeSYMGS_ref.cpp) on %d^3 (b = A u), %d iterations in %.2f s = "
+                      "%.3f s/iter, measured; scaled x%.0f rows to %dx%dx%d and x%d iterations "
+                      "(CG_ref's own count to 1e-10, %s)"
+                      % (sample_n, k, dt, per_it, scale, dims[0], dims[1], dims[2], iters, basis),
+            "measured_s_per_iteration": per_it, "sample_grid": [sample_n] * 3,
+            "extrapolation": {"rows_factor": scale, "iterations": iters, "iterations_basis": basis}}
 
 
 def run_reference(args, dims):
@@ -189,14 +222,13 @@ def run_reference(args, dims):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    iters = args.ref_iters
     vals = []
     cb = None
     for _ in range(args.warmup):
-        if cpu_reference_sample(iters, dims, sample_n=args.ref_sample, sample_it=1) is None:
+        if cpu_reference_sample(dims, sample_n=args.ref_sample, sample_it=1) is None:
             break
     for _ in range(max(1, args.steps)):
-        cb = cpu_reference_sample(iters, dims, sample_n=args.ref_sample, sample_it=args.ref_sample_it)
+        cb = cpu_reference_sample(dims, sample_n=args.ref_sample, sample_it=args.ref_sample_it)
         if cb is None:
             print(json.dumps({"impl": "reference",
                               "unavailable": "oracle/_ref/libhpcgref.so not built (needs the "
@@ -361,6 +393,65 @@ def run_varcoef(args):
     print(json.dumps(out))
 
 
+def run_slabs(args):
+    """Iterations to 1e-10 of the sharded solver against the number of z-slabs
+    (the reference's 1 x 1 x N process grid: SYMGS is block Jacobi across
+    slabs, src/ComputeSYMGS_ref.cpp:56, so the count depends on N).  One
+    global grid, split into N = 1, 2, 4, 8 slabs run as an in-process group on
+    one GPU (hpcgx_group_cg: halo planes as device copies, sums in rank order)
+    -- the algorithm of N GPUs, on one.  The system is the bench's b = A u,
+    u ~ U(-1, 1) seed 1, x0 = 0, both solvers."""
+    import torch
+    from hpcg_b200 import Group, Problem
+    from hpcg_b200._lib import CG_MG, CG_MIXED
+    g = args.grid
+    dims = (g[0], g[0], g[0]) if len(g) == 1 else tuple(g)
+    torch.cuda.set_device(0)
+    full = Problem(*dims)
+    full.generate("hpcg")
+    full.build_mixed()
+    u = full.fill_uniform(SEED_U, -1.0, 1.0)
+    b = full.spmv(u)
+    out = {"workload": "slabs", "grid": list(dims), "tolerance": TOL,
+           "system": "b = A u, u ~ U(-1,1) seed 1, x0 = 0", "slabs": {}}
+    x = torch.zeros_like(b)
+    row = {}
+    for name, f in (("fp64", full.cg), ("mixed", full.cg_mixed)):
+        x.zero_()
+        k, nr, nr0 = f(b, x, MAX_IT, TOL)
+        row[name] = k
+    out["slabs"]["1"] = dict(row, solver="one-GPU graph solver")
+    full.close()
+    del full
+    torch.cuda.empty_cache()
+    for N in (2, 4, 8):
+        if dims[2] % (N * 8):
+            continue
+        nz = dims[2] // N
+        ranks = [Problem(dims[0], dims[1], nz, nranks=N, rank=r) for r in range(N)]
+        for p in ranks:
+            p.generate("hpcg")
+            p.build_mixed()
+        grp = Group(ranks)
+        bs = [c.contiguous() for c in torch.split(b, b.numel() // N)]
+        row = {}
+        for name, mode in (("fp64", CG_MG), ("mixed", CG_MIXED)):
+            xs = [torch.zeros_like(c) for c in bs]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            k, nr, nr0 = grp.cg(bs, xs, MAX_IT, TOL, mode=mode)
+            torch.cuda.synchronize()
+            row[name] = k
+            row[name + "_rel_residual"] = nr / nr0
+        out["slabs"][str(N)] = dict(row, solver="in-process group of %d slabs of %dx%dx%d"
+                                    % (N, dims[0], dims[1], nz))
+        grp.close()
+        for p in ranks:
+            p.close()
+        torch.cuda.empty_cache()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -377,13 +468,14 @@ def main():
                     help="the sharded step-by-step solver with an NCCL communicator even on one GPU")
     ap.add_argument("--clocks-csv", default="",
                     help="keep the nvidia-smi clock samples here (%%d = rank)")
-    ap.add_argument("--ref-iters", type=int, default=0,
-                    help="iterations the reference arm scales to (0: measured FP64 count)")
-    ap.add_argument("--ref-sample", type=int, default=128)
-    ap.add_argument("--ref-sample-it", type=int, default=10)
-    ap.add_argument("--workload", default="pcg", choices=["pcg", "varcoef", "kernels"],
+    ap.add_argument("--ref-sample", type=int, default=256,
+                    help="grid (n^3) of the reference's timed CPU sample")
+    ap.add_argument("--ref-sample-it", type=int, default=3,
+                    help="CG_ref iterations timed per sample")
+    ap.add_argument("--workload", default="pcg", choices=["pcg", "varcoef", "kernels", "slabs"],
                     help="pcg: the headline metric; varcoef: the differentiable-solve checks; "
-                         "kernels: each plain operator on its own (give --grid 256)")
+                         "kernels: each plain operator on its own (give --grid 256); slabs: "
+                         "iterations against the number of z-slabs (give --grid 256)")
     ap.add_argument("--grid3", type=int, default=128)
     ap.add_argument("--grid4", type=int, nargs=3, default=[512, 512, 256])
     args = ap.parse_args()
@@ -393,12 +485,13 @@ def main():
     if args.workload == "kernels":
         run_kernels(args)
         return
+    if args.workload == "slabs":
+        run_slabs(args)
+        return
     g = args.grid
     dims = (g[0], g[0], g[0]) if len(g) == 1 else tuple(g)
 
     if args.impl == "reference":
-        if args.ref_iters <= 0:
-            args.ref_iters = REF_ITERS_DEFAULT.get(dims, 300)
         run_reference(args, dims)
         return
 
@@ -420,7 +513,7 @@ def main():
     torch.cuda.set_device(dev)
 
     from hpcg_b200 import Problem, nccl_unique_id
-    from hpcg_b200._lib import PROBE_GS_FINE, PROBE_GS_FINE_BWD, PROBE_SPMV_FINE
+    from hpcg_b200._lib import CG_MG, CG_MIXED, PROBE_GS_FINE, PROBE_GS_FINE_BWD, PROBE_SPMV_FINE
 
     def barrier():
         torch.cuda.synchronize()
@@ -508,30 +601,71 @@ def main():
         torch.cuda.synchronize()
         t64.append(e0.elapsed_time(e1) * 1e-3)
     t_fp64 = statistics.mean(t64)
+    # bytes of one iteration as this implementation moves them (one-GPU
+    # solver; read while each solver's iteration graph is current)
+    ib = {}
+    if not sharded:
+        ib = {"mixed": P.iteration_bytes(CG_MIXED), "fp64": P.iteration_bytes(CG_MG)}
     x64 = x.clone()
     true_fp64 = gnorm(b - P.spmv(x64)) / gnorm(b)
     x_diff = gnorm(x_mixed - x64) / gnorm(x64)
     err_u = gnorm(x_mixed - u) / gnorm(u)
 
-    # ---------------- end to end through the C ABI from pinned host buffers
+    # ---------------- FP64 with the mixed solver's column derivation: the FP64
+    # solve that differs from the mixed one in precision only (every column
+    # from the stencil offsets, no int32 column reads)
+    P.set_stencil_columns(True)
+    solve(False)
+    t64s = []
+    for _ in range(max(1, args.fp64_steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        k64s, nr64s, nr064s = solve(False)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize()
+        t64s.append(e0.elapsed_time(e1) * 1e-3)
+    t_fp64s = statistics.mean(t64s)
+    x64s_diff = gnorm(x - x64) / gnorm(x64)
+    if not sharded:
+        ib["fp64_stencil_cols"] = P.iteration_bytes(CG_MG)
+    P.set_stencil_columns(False)
+
+    # ---------------- end to end through the C ABI from pinned host buffers:
+    # b copied in and x copied out inside each timed solve
     bh = b.cpu().pin_memory()
     xh = torch.zeros(n, dtype=torch.float64).pin_memory()
-    barrier()
-    te = time.perf_counter()
-    ke, nre, nr0e = P.cg_host(bh.numpy(), xh.numpy(), MAX_IT, TOL, mixed=True)
-    torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - te
+    P.cg_host(bh.numpy(), xh.numpy(), MAX_IT, TOL, mixed=True)   # untimed warm-up
+    te2e = []
+    for _ in range(args.steps):
+        xh.zero_()
+        barrier()
+        te = time.perf_counter()
+        ke, nre, nr0e = P.cg_host(bh.numpy(), xh.numpy(), MAX_IT, TOL, mixed=True)
+        torch.cuda.synchronize()
+        te2e.append(time.perf_counter() - te)
+    t_e2e = statistics.mean(te2e)
 
     # ---------------- max over ranks
-    t_mixed, t_fp64, t_e2e = max_over_ranks([t_mixed, t_fp64, t_e2e], dist, f"cuda:{dev}")
+    t_mixed, t_fp64, t_fp64s, t_e2e = max_over_ranks([t_mixed, t_fp64, t_fp64s, t_e2e], dist,
+                                                     f"cuda:{dev}")
 
     flops, b64, b32, n0, z0 = model(dims)
     peak, peak_kind = peaks()
     # whole job: every rank does one slab's (or one replica's) work per iteration
     gf_mixed = world * flops * iters_mixed[-1] / t_mixed / 1e9
     gf_fp64 = world * flops * k64 / t_fp64 / 1e9
-    hbm_mixed = world * b32 * iters_mixed[-1] / t_mixed / 1e9
-    hbm_fp64 = world * b64 * k64 / t_fp64 / 1e9
+    ref_mixed = world * b32 * iters_mixed[-1] / t_mixed / 1e9
+    ref_fp64 = world * b64 * k64 / t_fp64 / 1e9
+
+    def whole_iteration(kind, iters, t):
+        if kind not in ib:
+            return None
+        ach = world * ib[kind] * iters / t / 1e9
+        return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "bytes_per_iteration": ib[kind], "iterations": iters, "time_s": t,
+                "peak_kind": peak_kind}
     traffic = {}
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic_%d.json" % dims[0])
     if os.path.exists(tpath) and dims[0] == dims[1] == dims[2]:
@@ -557,7 +691,7 @@ def main():
     cpu = None
     if not args.no_cpu and world == 1:   # the CPU sample is taken at N = 1 only
         try:
-            cpu = cpu_reference_sample(k64, dims)
+            cpu = cpu_reference_sample(dims)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"unavailable": str(e)}
     clocks = clk.summary(dev)
@@ -570,20 +704,35 @@ def main():
         "iterations": {"mixed": iters_mixed[-1], "fp64": k64},
         "fp64_time_s": t_fp64,
         "speedup_mixed_vs_fp64": t_fp64 / t_mixed,
+        "fp64_stencil_cols_time_s": t_fp64s,
+        "speedup_mixed_vs_fp64_stencil_cols": t_fp64s / t_mixed,
+        "fp64_stencil_cols": {"iterations": k64s, "x_rel_diff_vs_fp64": x64s_diff,
+                              "note": "FP64 PCG with every column derived from the stencil "
+                                      "offsets, as the mixed solver does: the mixed-vs-FP64 "
+                                      "ratio from precision alone"},
         "fp64_rel_residual": {"mixed_recursive": relres_mixed, "mixed_true": true_mixed,
                               "fp64_true": true_fp64},
         "x_rel_diff_vs_fp64": x_diff, "x_rel_err_vs_u": err_u,
         "gflops": {"mixed": gf_mixed, "fp64": gf_fp64, "model": "src/ReportResults.cpp:81-97"},
-        "hbm_effective": {"mixed_gbs": hbm_mixed, "fp64_gbs": hbm_fp64,
-                          "model": "bytes per iteration of the reference implementation's steps "
-                                   "(SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n, R+P 40 n_c, CG "
-                                   "vectors 112 n; mixed V-cycle 6 B/nnz and FP32 vectors) / time",
-                          "peak_gbs": peak, "peak_kind": peak_kind},
+        "roofline_iteration": {
+            "mixed": whole_iteration("mixed", iters_mixed[-1], t_mixed),
+            "fp64": whole_iteration("fp64", k64, t_fp64),
+            "fp64_stencil_cols": whole_iteration("fp64_stencil_cols", k64s, t_fp64s),
+            "model": "this implementation's algorithmic bytes per CG iteration "
+                     "(hpcgx_iteration_bytes: every launch of the iteration, real nonzeros, each "
+                     "vector element once per launch) x iterations / solve time"},
+        "reference_model_gbs": {"mixed": ref_mixed, "fp64": ref_fp64,
+                                "model": "bytes per iteration of the reference implementation's "
+                                         "steps (SpMV 12 nnz + 16 n, SYMGS 24 nnz + 48 n, R+P "
+                                         "40 n_c, CG vectors 112 n; mixed V-cycle 6 B/nnz, FP32 "
+                                         "vectors) / time: work this design does not do, so it "
+                                         "exceeds the HBM peak; for comparison with other HPCG "
+                                         "implementations only"},
         "roofline": roofline(PROBE_SPMV_FINE, "k_spmv<double,double,1,1>"),
         "roofline_gs_bwd": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f64>"),
         "roofline_gs_fine_all_modes": roofline(PROBE_GS_FINE, "k_gs_class finest level, all modes"),
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": world * 2 * n * 8,
-                "d2h_bytes_per_step": world * n * 8},
+                "d2h_bytes_per_step": world * n * 8, "steps": args.steps},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -593,14 +742,6 @@ def main():
     P.close()
     if dist:
         dist.destroy_process_group()
-
-
-# Iterations the reference arm scales its per-iteration sample to when run on
-# its own: the FP64 PCG iteration count this build measured on the same
-# system to 1e-10 (bench runs on B200: 295 at 512^3, 170 at 256^3); the
-# reference's natural-order smoother is not run at 512^3 because its int32
-# counters overflow there.
-REF_ITERS_DEFAULT = {(512, 512, 512): 295, (256, 256, 256): 170}
 
 
 if __name__ == "__main__":

@@ -38,7 +38,11 @@ SIGNATURES = {
     "hpcgx_load_level_rows": (_I, [_P, _I, _P, _P, _P]),
     "hpcgx_check_f2c": (_I, [_P, _I, _P, _I64]),
     "hpcgx_generate": (_I, [_P, _I, _U64, _D]),
+    "hpcgx_create_general": (_I, [_I, _I, _P]),
+    "hpcgx_load_level_general": (_I, [_P, _I, _I64, _P, _P, _P, _P, _I64]),
+    "hpcgx_colours": (_I, [_P, _I]),
     "hpcgx_build_mixed": (_I, [_P]),
+    "hpcgx_set_stencil_columns": (_I, [_P, _I]),
     "hpcgx_set_diagonal_host": (_I, [_P, _I, _P]),
     "hpcgx_get_diagonal_host": (_I, [_P, _I, _P]),
     "hpcgx_set_values": (_I, [_P, _I, _P, _I]),
@@ -72,6 +76,7 @@ SIGNATURES = {
     "hpcgx_set_probe": (_I, [_P, _I]),
     "hpcgx_probe_read": (_I, [_P, _I, _DP, _I64P, _DP, _I]),
     "hpcgx_launch_count": (_I64, [_P]),
+    "hpcgx_iteration_bytes": (_I, [_P, _I, _DP]),
     "hpcgx_synchronize": (_I, [_P]),
     "hpcgx_set_stream": (_I, [_P, _P]),
     "hpcgx_create_slab": (_I, [_I, _I, _I, _I, _I, _I, _I, C.POINTER(_P)]),
@@ -79,7 +84,6 @@ SIGNATURES = {
     "hpcgx_attach_nccl": (_I, [_P, _P, _I]),
     "hpcgx_attach_comm": (_I, [_P, HALO_FN, SUM_FN, _P]),
     "hpcgx_check_status": (_I, []),
-    "hpcgx_wave_schedule": (_I, [_I, _I, _I, _I, _I, _I, _IP, _IP, _IP, _IP, _IP, _IP]),
     "hpcgx_group_create": (_I, [_P, _I, C.POINTER(_P)]),
     "hpcgx_group_destroy": (_I, [_P]),
     "hpcgx_group_spmv": (_I, [_P, _I, _P, _P]),

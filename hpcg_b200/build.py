@@ -15,8 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libhpcgx.so")
 LIB_CHECKED = os.path.join(HERE, "libhpcgx_checked.so")   # -DHPCGX_CHECKED: index-checked kernels
-SOURCES = ["kernels.cu", "problem.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "kernels.cuh"]
+SOURCES = ["kernels.cu", "problem.cu", "noalloc.cu", "general.cu"]
+HEADERS = ["common.cuh", "kernels.cuh", "general.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]

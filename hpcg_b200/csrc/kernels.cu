@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <type_traits>
 
 namespace hpcgx {
@@ -536,6 +537,30 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 
 // ---------------------------------------------------------------- Gauss-Seidel
 
+// Per-thread sums of a GS_DOT launch: r.z and z.Ap over the rows it finalises.
+struct RzAcc {
+  double rz = 0.0, zap = 0.0;
+};
+
+// End of a GS_DOT launch: the block's sums join the grid reduction; launch
+// slot 3's last block adds the four launches' totals in slot order and runs
+// CG's beta step.
+__device__ __forceinline__ void rz_finish(const RzFuse &f, const RzAcc &acc) {
+  double v[2] = {acc.rz, acc.zap}, tot[2];
+  if (grid_reduce<2>(v, f.red, tot) && threadIdx.x == 0) {
+    if (f.slot < 3) {
+      f.part[2 * f.slot] = tot[0];
+      f.part[2 * f.slot + 1] = tot[1];
+    } else {
+      double t[2];
+      t[0] = ((__ldcg(f.part) + __ldcg(f.part + 2)) + __ldcg(f.part + 4)) + tot[0];
+      t[1] = ((__ldcg(f.part + 1) + __ldcg(f.part + 3)) + __ldcg(f.part + 5)) + tot[1];
+      finish_or_defer<2>(f.red, FIN_CG_RZ, f.st, t);
+    }
+  }
+}
+
+
 // One Gauss-Seidel row update, src/ComputeSYMGS_ref.cpp:72-80:
 //   sum = r_i - sum_j a_ij x_j (diagonal included, slot order); sum += x_i a_ii;
 //   x_i = sum / a_ii.
@@ -558,10 +583,17 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 //       its backward update (the first step of the backward sweep): between
 //       the two only x_i changes, so the backward value is recomputed from the
 //       same registers and only that value is stored.
-template <bool ZERO, bool PRO, bool RES, bool SYM = false, class VT, class T, class RT>
+// VEC (FP32 x, even nx, 8-byte aligned x): an interior row reads the three x
+//       neighbours on each of its 9 neighbouring x-lines with one 8-byte load
+//       of the aligned pair among them and one 4-byte load of the third.
+// DOT:  the new x_i is final (a GS_DOT launch): r_i x_i and, with ap, x_i ap_i
+//       are added to acc.
+template <bool ZERO, bool PRO, bool RES, bool SYM = false, bool STN = false, bool DOT = false,
+          bool VEC = false, class VT, class T, class RT>
 __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, int c,
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
-                                       T *__restrict__ rc) {
+                                       T *__restrict__ rc, RzAcc *acc = nullptr,
+                                       const double *__restrict__ ap = nullptr) {
   RowId id = id0;
   check_row(A, id, 3);
   int32_t col[HPCGX_STENCIL];
@@ -569,8 +601,9 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
   // slots whose neighbour is read: all, or (zero guess) the lower colours
   auto need = [c](int s) { return !ZERO || s == HPCGX_DIAG_SLOT || ((c ^ slot_mask(s)) < c); };
   // The mixed V-cycle (BF16 values) derives its columns from the stencil
-  // offsets; the FP64 path reads the stored int32 columns.
-  constexpr bool IMPLICIT = std::is_same<VT, uint16_t>::value;
+  // offsets; the FP64 path reads the stored int32 columns, or derives them
+  // too (STN, the FP64 solve with stencil columns).
+  constexpr bool IMPLICIT = STN || std::is_same<VT, uint16_t>::value;
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
     load_vals(A.vals, id.k, p, need, val + 9 * p);
@@ -578,7 +611,8 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
   }
   if (IMPLICIT) stencil_cols<true>(A, id, need, col);
   check_cols(A, col, need, 4);
-  const T rhs = vec_to(__ldg(r + id.row), T());
+  const RT rraw = __ldg(r + id.row);
+  const T rhs = vec_to(rraw, T());
   int64_t crow = 0;
   if (PRO || RES) {
     const int nxc = A.nx >> 1, nyc = A.ny >> 1;
@@ -592,11 +626,41 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
   // is skipped below.  The gather itself does not wait for the value: every
   // column is in range.
   T xv[HPCGX_STENCIL];
+  bool gathered = false;
+  if constexpr (VEC && std::is_same<T, float>::value) {
+    const bool interior = id.ix > 0 && id.ix + 1 < A.nx && id.iy > 0 && id.iy + 1 < A.ny &&
+                          (id.iz > 0 || A.zlo) && (id.iz + 1 < A.nz || A.zhi);
+    if (interior) {
+      const int px = c & 1, r32 = (int)id.row;
 #pragma unroll
-  for (int s = 0; s < HPCGX_STENCIL; ++s) {
-    if (s == HPCGX_DIAG_SLOT) continue;
-    if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
-    xv[s] = x[col[s]];
+      for (int ln = 0; ln < 9; ++ln) {
+        // zero guess: a line other than the row's own is read if its colours
+        // are lower; on the own line the x-neighbours are of colour c ^ 1
+        const bool used = ln == 4 ? (!ZERO || (c & 1)) : need(3 * ln);
+        if (!used) continue;
+        const int b = r32 + A.off[3 * ln + 1];   // the neighbour with dx = 0
+        if (px == 0) {
+          const float2 v = *reinterpret_cast<const float2 *>(x + b);
+          xv[3 * ln] = x[b - 1];
+          xv[3 * ln + 1] = v.x;
+          xv[3 * ln + 2] = v.y;
+        } else {
+          const float2 v = *reinterpret_cast<const float2 *>(x + b - 1);
+          xv[3 * ln] = v.x;
+          xv[3 * ln + 1] = v.y;
+          xv[3 * ln + 2] = x[b + 1];
+        }
+      }
+      gathered = true;
+    }
+  }
+  if (!gathered) {
+#pragma unroll
+    for (int s = 0; s < HPCGX_STENCIL; ++s) {
+      if (s == HPCGX_DIAG_SLOT) continue;
+      if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
+      xv[s] = x[col[s]];
+    }
   }
   T sum = rhs;
   const T d = val[HPCGX_DIAG_SLOT];
@@ -623,10 +687,19 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
       sum2 = mac_sub(sum2, val[s], xv[s]);
     }
     sum2 = mac_add(sum2, xn, d);
-    x[id.row] = rn_div(sum2, d);
+    const T xb = rn_div(sum2, d);
+    x[id.row] = xb;
+    if (DOT) {
+      acc->rz += (double)rraw * (double)xb;
+      if (ap) acc->zap += (double)xb * __ldg(ap + id.row);
+    }
     return;
   }
   x[id.row] = xn;
+  if (DOT) {
+    acc->rz += (double)rraw * (double)xn;
+    if (ap) acc->zap += (double)xn * __ldg(ap + id.row);
+  }
   if (RES) {
     T ax = T(0);
 #pragma unroll
@@ -640,10 +713,16 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
 // 2Q then 2Q+1 (DIR = 0) or 2Q+1 then 2Q (DIR = 1).  A block owns whole lines,
 // so the x-neighbours of a row (the other colour of the class) are its own.
 // PRO / RES act on colour 0 only.
-template <bool ZERO, bool PRO, bool RES, int Q, int DIR, class VT, class T, class RT>
+template <int MODE, int Q, int DIR, class VT, class T, class RT>
 __device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo &C, int j0, int j1,
                                          const RT *__restrict__ r, T *x,
-                                         const T *__restrict__ xc, T *__restrict__ rc) {
+                                         const T *__restrict__ xc, T *__restrict__ rc,
+                                         const RzFuse &rz) {
+  constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0, PRO = (MODE & GS_PROLONG) != 0,
+                 RES = (MODE & GS_RESTRICT) != 0, STN = (MODE & GS_STENCIL) != 0,
+                 DOT = (MODE & GS_DOT) != 0, VEC = (MODE & GS_VEC) != 0;
+  RzAcc acc;
+  const double *ap = (DOT && rz.flex && rz.st->k > 1) ? rz.Ap : nullptr;
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
     const int px = DIR ? 1 - half : half;
@@ -652,12 +731,13 @@ __device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo 
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
       const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
       if ((PRO || RES) && c == 0)
-        gs_row<ZERO, PRO, RES>(A, id, c, r, x, xc, rc);
+        gs_row<ZERO, PRO, RES, false, STN, false, VEC>(A, id, c, r, x, xc, rc);
       else
-        gs_row<ZERO, false, false>(A, id, c, r, x, xc, rc);
+        gs_row<ZERO, false, false, false, STN, DOT, VEC>(A, id, c, r, x, xc, rc, &acc, ap);
     }
     if (half == 0) __syncthreads();
   }
+  if (DOT) rz_finish(rz, acc);
 }
 
 // The last class of a forward sweep fused with the first class of the
@@ -667,24 +747,31 @@ __device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo 
 // lines carry every dependency; the matrix rows of the class are read from
 // DRAM once instead of twice (colour 6's rows come back from L2 in the last
 // phase).
-template <bool ZERO, class VT, class T, class RT>
+// DOT: colours 7 and 6 are final after their backward updates (phases 2, 3).
+template <int MODE, class VT, class T, class RT>
 __device__ __forceinline__ void gs_lines_sym3(const LevelMat<VT> &A, const ClassInfo &C, int j0,
-                                              int j1, const RT *__restrict__ r, T *x) {
+                                              int j1, const RT *__restrict__ r, T *x,
+                                              const RzFuse &rz) {
+  constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0, STN = (MODE & GS_STENCIL) != 0,
+                 DOT = (MODE & GS_DOT) != 0, VEC = (MODE & GS_VEC) != 0;
+  RzAcc acc;
+  const double *ap = (DOT && rz.flex && rz.st->k > 1) ? rz.Ap : nullptr;
   const int cnt0 = (j1 - j0) * C.len[0], cnt1 = (j1 - j0) * C.len[1];
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
-    gs_row<ZERO, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
-                               (T *)nullptr);
+    gs_row<ZERO, false, false, false, STN, false, VEC>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r,
+                                                       x, (const T *)nullptr, (T *)nullptr);
   __syncthreads();
   for (int t = threadIdx.x; t < cnt1; t += blockDim.x)
-    gs_row<ZERO, false, false, true>(A, row_of(C, A.nx, A.ny, 1, j0, t), 7, r, x,
-                                     (const T *)nullptr, (T *)nullptr);
+    gs_row<ZERO, false, false, true, STN, DOT, VEC>(A, row_of(C, A.nx, A.ny, 1, j0, t), 7, r, x,
+                                                    (const T *)nullptr, (T *)nullptr, &acc, ap);
   __syncthreads();
   // Colour 6 backward multiplies every slot; after a zero-guess forward part,
   // rows of colours 6 and 7 in other blocks may still be unwritten, which the
   // exact columns of slots without a neighbour never reach.
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
-    gs_row<false, false, false>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x, (const T *)nullptr,
-                                (T *)nullptr);
+    gs_row<false, false, false, false, STN, DOT, VEC>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x,
+                                                      (const T *)nullptr, (T *)nullptr, &acc, ap);
+  if (DOT) rz_finish(rz, acc);
 }
 
 // A half sweep over one class, lpb lines per block.  MODE bits:
@@ -695,191 +782,32 @@ __device__ __forceinline__ void gs_lines_sym3(const LevelMat<VT> &A, const Class
 // 256-thread blocks per SM; the BF16 sweeps read 2 B per slot and are latency
 // bound, so they are held to 64 registers for four blocks per SM (five,
 // at 48 registers, spill and run slower).
-template <class VT>
-constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 4 : 2; }
+// The GS_DOT launches (four per V-cycle) keep two FP64 sums per thread and
+// run at three blocks per SM rather than spill.
+template <class VT, int MODE = 0>
+constexpr int gs_min_blocks() {
+  return std::is_same<VT, uint16_t>::value ? ((MODE & GS_DOT) ? 3 : 4) : 2;
+}
 
 template <int MODE, int DIR, int QS, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT, MODE>())
 k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
+           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done,
+           RzFuse rz) {
   if (done && *done) return;
   const int j0 = blockIdx.x * lpb;
   const int j1 = min(j0 + lpb, C.lines);
-  gs_lines<(MODE & GS_ZERO_GUESS) != 0, (MODE & GS_PROLONG) != 0, (MODE & GS_RESTRICT) != 0, QS,
-           DIR>(A, C, j0, j1, r, x, xc, rc);
+  gs_lines<MODE, QS, DIR>(A, C, j0, j1, r, x, xc, rc, rz);
 }
 
-template <bool ZERO, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
+template <int MODE, class VT, class T, class RT>
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT, MODE>())
 k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-                const int *__restrict__ done) {
+                const int *__restrict__ done, RzFuse rz) {
   if (done && *done) return;
   const int j0 = blockIdx.x * lpb;
   const int j1 = min(j0 + lpb, C.lines);
-  gs_lines_sym3<ZERO>(A, C, j0, j1, r, x);
-}
-
-// ---------------------------------------------------------------- one-launch sweep
-//
-// A whole symmetric sweep of one level in one launch.  The seven class steps
-// of the class launches -- forward classes 0, 1, 2, class 3 forward and
-// backward, backward classes 2, 1, 0 -- become stages 0..6 of a wavefront
-// over the z-planes.  A work item is a run of lines of one stage's class in
-// one z-plane (classes 0 and 1 live on even planes, 2 and 3 on odd ones).
-//
-// Order: stage s may start plane z once stage s-1 has finished every one of
-// the planes z-1, z, z+1 that holds its class.  Then every earlier stage has
-// finished those planes (by induction), so the rows the item reads hold the
-// values they hold in the class launches: a row of an earlier colour its new
-// value, a row of a later colour its old one, since a later stage reaches a
-// plane next to z only after this stage finished z.  Within a colour the
-// rows are independent, so the sweep is bit-identical to the class launches.
-//
-// Scheduling: items carry tickets sorted by key = z + lag * s (lag >= 2), so
-// every item an item waits for has a smaller ticket.  Blocks take tickets
-// from a counter and only wait for tickets already taken by running blocks;
-// the waits end whatever the number of co-resident blocks.  A finished item
-// adds one to its (stage, plane) counter with release semantics; a waiting
-// block's first thread reads the counters with acquire semantics, then the
-// block synchronises, so the whole block sees the finished rows.  Every wait
-// gives up after kWaveSpin polls, records a fault (read by the host) and
-// stops the launch's remaining items.  The last block to leave resets the
-// counters for the next launch.
-//
-// What it was for: each class launch reads the x-neighbourhood of its rows in
-// all z-planes, i.e. the whole x vector, from DRAM; a wavefront could keep the
-// planes between a plane's first and last stage in L2.  Measured on B200 at
-// 512^3 (mixed V-cycle, finest level) the matrix values streaming past in
-// between (~0.9 GB) evict them -- DRAM traffic per sweep is no lower than the
-// class launches' -- and the per-item serial steps lower the DRAM rate:
-// 3.79 ms per symmetric sweep at lag 6 and 2048-row items against 3.32 ms.
-// So it is an option (HPCGX_GS_WAVE=1), not the default.
-
-struct WaveDev {
-  const int2 *tab;   // (stage << 16 | class plane, first ticket), ticket order
-  int *ctr;          // [7][nzq] finished items; then ticket, exits, abort
-  int ntab, total, lpi, nzq, nz;
-  int ipp[4];        // items per plane of each class
-  int uniform;       // > 0: every entry has this many items (entry = ticket / uniform)
-};
-
-__device__ unsigned int g_wave_fault = 0u;
-constexpr int kWaveSpin = 1 << 22;
-constexpr int kWaveSmemEntries = 4096;   // 16 KB of shared memory per block at most
-
-__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void red_release_gpu(int *p, int v) {
-  asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__host__ __device__ constexpr int wave_class(int s) { return s <= 3 ? s : 6 - s; }
-
-// First thread only: waits until stage s-1 has finished the planes next to iz.
-__device__ bool wave_wait(const WaveDev &W, int s, int iz) {
-  const int p = s - 1, qp = wave_class(p), pzp = qp >> 1;
-  const int need = qp == 0 ? W.ipp[0] : qp == 1 ? W.ipp[1] : qp == 2 ? W.ipp[2] : W.ipp[3];
-  int *abortf = W.ctr + 7 * W.nzq + 2;
-  for (int z = iz - 1; z <= iz + 1; ++z) {
-    if (z < 0 || z >= W.nz || (z & 1) != pzp) continue;
-    const int *c = W.ctr + p * W.nzq + ((z - pzp) >> 1);
-    for (int polls = 0; ld_acquire_gpu(c) < need; ++polls) {
-      if (polls >= kWaveSpin) atomicOr(&g_wave_fault, 1u);
-      if (polls >= kWaveSpin || *(volatile int *)abortf) {
-        atomicExch(abortf, 1);
-        return false;
-      }
-      __nanosleep(128);
-    }
-  }
-  return true;
-}
-
-template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
-k_gs_wave(LevelMat<VT> A, ClassSet CS, WaveDev W, const RT *__restrict__ r, T *x,
-          const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
-  if (done && *done) return;
-  __shared__ int item[3];
-  // uniform tables are decoded from shared memory: entry = ticket / uniform
-  extern __shared__ int tab_code[];
-  const bool stab = W.uniform > 0 && W.ntab <= kWaveSmemEntries;
-  if (stab) {
-    for (int i = threadIdx.x; i < W.ntab; i += blockDim.x) tab_code[i] = W.tab[i].x;
-    __syncthreads();
-  }
-  int *ticket = W.ctr + 7 * W.nzq;
-  // The first thread holds the ticket of the next item while the block works
-  // on the current one, so that the atomic's latency is hidden (the held
-  // ticket is larger than the current one, which never waits for it).
-  int next = 0;
-  if (threadIdx.x == 0) next = atomicAdd(ticket, 1);
-  for (;;) {
-    if (threadIdx.x == 0) {
-      int s = -1, jz = 0, b = 0;
-      const int t = next;
-      if (t < W.total && !*(volatile int *)(ticket + 2)) {
-        int2 e;
-        if (stab) {
-          const int i = t / W.uniform;
-          e = make_int2(tab_code[i], i * W.uniform);
-        } else if (W.uniform > 0) {
-          e = W.tab[t / W.uniform];
-        } else {
-          int lo = 0, hi = W.ntab - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (W.tab[mid].y <= t) lo = mid; else hi = mid - 1;
-          }
-          e = W.tab[lo];
-        }
-        s = e.x >> 16;
-        jz = e.x & 0xffff;
-        b = t - e.y;
-        if (s > 0 && !wave_wait(W, s, (wave_class(s) >> 1) + 2 * jz)) s = -1;
-        if (s >= 0) next = atomicAdd(ticket, 1);
-      }
-      item[0] = s;
-      item[1] = jz;
-      item[2] = b;
-    }
-    __syncthreads();
-    const int s = item[0], jz = item[1], b = item[2];
-    if (s < 0) break;
-    const int nyq = s == 0 || s == 6 ? CS.c[0].nyq : s == 1 || s == 5 ? CS.c[1].nyq
-                  : s == 2 || s == 4 ? CS.c[2].nyq : CS.c[3].nyq;
-    const int j0 = jz * nyq + b * W.lpi;
-    const int j1 = min(j0 + W.lpi, (jz + 1) * nyq);
-    switch (s) {
-      case 0: gs_lines<ZERO, PRO, false, 0, 0>(A, CS.c[0], j0, j1, r, x, xc, rc); break;
-      case 1: gs_lines<ZERO, false, false, 1, 0>(A, CS.c[1], j0, j1, r, x, xc, rc); break;
-      case 2: gs_lines<ZERO, false, false, 2, 0>(A, CS.c[2], j0, j1, r, x, xc, rc); break;
-      case 3: gs_lines_sym3<ZERO>(A, CS.c[3], j0, j1, r, x); break;
-      case 4: gs_lines<false, false, false, 2, 1>(A, CS.c[2], j0, j1, r, x, xc, rc); break;
-      case 5: gs_lines<false, false, false, 1, 1>(A, CS.c[1], j0, j1, r, x, xc, rc); break;
-      default: gs_lines<false, false, RES, 0, 1>(A, CS.c[0], j0, j1, r, x, xc, rc); break;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) red_release_gpu(W.ctr + s * W.nzq + jz, 1);
-  }
-  // the last block to leave resets the counters for the next launch
-  __shared__ int last;
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(ticket + 1, 1) == (int)gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last) {
-    __threadfence();
-    for (int i = threadIdx.x; i < 7 * W.nzq; i += blockDim.x) W.ctr[i] = 0;
-    if (threadIdx.x == 0) {
-      ticket[0] = 0;
-      ticket[1] = 0;
-      ticket[2] = 0;
-    }
-  }
+  gs_lines_sym3<MODE>(A, C, j0, j1, r, x, rz);
 }
 
 // Residual restricted at the injected points (colour 0: even ix, iy, iz):
@@ -960,15 +888,18 @@ k_waxpby(int64_t n, double alpha, const double *__restrict__ x, double beta,
   }
 }
 
+// x.y; the last block stores the total (FIN_STORE into target) or runs a CG
+// scalar step on it (target: the CgState).
 __global__ void __launch_bounds__(kThreads)
-k_dot(int64_t n, const double *__restrict__ x, const double *__restrict__ y, Reduce red,
-      double *out) {
+k_dot(int64_t n, const double *__restrict__ x, const double *__restrict__ y, Reduce red, int fin,
+      void *target, const int *__restrict__ done) {
+  if (done && *done) return;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   double acc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride)
     acc += x[i] * y[i];
   double v[1] = {acc}, tot[1];
-  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) out[0] = tot[0];
+  if (grid_reduce<1>(v, red, tot) && threadIdx.x == 0) finish_or_defer<1>(red, fin, target, tot);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -1502,6 +1433,7 @@ int launch_get_diagonal(const LevelDev &L, double *diag, cudaStream_t s) {
 int launch_spmv(const LevelDev &L, const double *x, double *y, const Reduce *dot, int fin,
                 void *fin_target, const int *done, cudaStream_t s, bool implicit_cols) {
   if (L.spmv_blocks == 0) return 0;
+  implicit_cols = implicit_cols || L.stencil_cols;
   // measured at 512^3: two line groups per block help the stencil-column
   // SpMV (4.77 against 5.11 ms with the fused dot product), not the other
   const ClassSet cs = classes_of(L, implicit_cols ? 2 : 1);
@@ -1543,46 +1475,88 @@ struct ValsOf<float> {
   static const uint16_t *get(const LevelDev &L) { return L.vals16; }
 };
 
-template <class T, class RT>
-int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                    const T *xc, T *rc, const int *done, cudaStream_t s) {
+// The class kernels.  EXTRA: GS_STENCIL (FP64: columns from the stencil
+// offsets) or GS_VEC (FP32 x: paired x gathers), added to every launch's mode.
+template <int EXTRA, class T, class RT>
+int launch_gs_rows(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
+                   const T *xc, T *rc, const int *done, cudaStream_t s, const RzFuse *rzp) {
   using VT = typename ValsOf<T>::VT;
-  if (L.blocks[q] == 0) return 0;
   const LevelMat<VT> A = mat_of(L, ValsOf<T>::get(L));
   const dim3 g(L.blocks[q]), b(L.threads[q]);
   const int lpb = L.lines_per_block[q];
   const ClassInfo &C = L.cls[q];
+  const RzFuse rz = rzp ? *rzp : RzFuse();
+  if (mode & GS_DOT) {
+    // the mixed V-cycle's last four finest-level launches (no FP64 variants)
+    if constexpr (std::is_same<T, float>::value) {
+      if (!rzp) return 0;
+      if (mode == (GS_SYM3 | GS_DOT) && q == 3) {
+        k_gs_class3_sym<GS_DOT | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done, rz);
+        return 1;
+      }
+      if (mode == (GS_PLAIN | GS_DOT) && backward) {
+        k_gs_class<GS_DOT | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
+        return 1;
+      }
+    }
+    return 0;
+  }
   if (mode & GS_SYM3) {
     if (q != 3) return 0;
     if (mode & GS_ZERO_GUESS)
-      k_gs_class3_sym<true><<<g, b, 0, s>>>(A, C, lpb, r, x, done);
+      k_gs_class3_sym<GS_ZERO_GUESS | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done, rz);
     else
-      k_gs_class3_sym<false><<<g, b, 0, s>>>(A, C, lpb, r, x, done);
+      k_gs_class3_sym<GS_PLAIN | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done, rz);
     return 1;
   }
   if (mode == GS_ZERO_GUESS && !backward) {
     switch (q) {
-      case 0: k_gs_class<GS_ZERO_GUESS, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
-      case 1: k_gs_class<GS_ZERO_GUESS, 0, 1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
-      case 2: k_gs_class<GS_ZERO_GUESS, 0, 2><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
-      default: k_gs_class<GS_ZERO_GUESS, 0, 3><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      case 0: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
+      case 1: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
+      case 2: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 2><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
+      default: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 3><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
     }
     return 1;
   }
   if (mode == GS_RESTRICT && backward && q == 0) {
-    k_gs_class<GS_RESTRICT, 1, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_RESTRICT | EXTRA, 1, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
     return 1;
   }
   if (mode == GS_PROLONG && !backward && q == 0) {
-    k_gs_class<GS_PROLONG, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_PROLONG | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
     return 1;
   }
   if (mode != GS_PLAIN) return 0;
   if (backward)
-    k_gs_class<GS_PLAIN, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_PLAIN | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
   else
-    k_gs_class<GS_PLAIN, 0, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_PLAIN | EXTRA, 0, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
   return 1;
+}
+
+// HPCGX_VEC_GATHER=0 keeps the one-load-per-neighbour gathers of the mixed
+// sweeps (the paired gathers are the default where they apply).
+bool vec_gathers_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("HPCGX_VEC_GATHER");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+template <class T, class RT>
+int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
+                    const T *xc, T *rc, const int *done, cudaStream_t s, const RzFuse *rz) {
+  if (L.blocks[q] == 0) return 0;
+  if constexpr (std::is_same<T, double>::value) {
+    if (L.stencil_cols)
+      return launch_gs_rows<GS_STENCIL>(L, q, backward, mode, r, x, xc, rc, done, s, rz);
+  } else {
+    // paired gathers: x-lines start on even rows and x is 8-byte aligned
+    if (vec_gathers_enabled() && L.nx % 2 == 0 && ((uintptr_t)x & 7) == 0)
+      return launch_gs_rows<GS_VEC>(L, q, backward, mode, r, x, xc, rc, done, s, rz);
+  }
+  return launch_gs_rows<0>(L, q, backward, mode, r, x, xc, rc, done, s, rz);
 }
 
 template <class T, class RT>
@@ -1617,114 +1591,6 @@ template int launch_prolong<double>(const LevelDev &, int64_t, const double *, d
 template int launch_prolong<float>(const LevelDev &, int64_t, const float *, float *, const int *,
                                    cudaStream_t);
 
-std::vector<int2> wave_plan(LevelDev &L, int lag, int rows_per_item) {
-  std::vector<int2> tab;
-  L.wave_ntab = L.wave_total = L.wave_lpi = L.wave_nzq = 0;
-  for (int q = 0; q < 4; ++q) L.wave_ipp[q] = 0;
-  const int nzq = (L.nz + 1) / 2;
-  // every class needs lines on its planes (ny, nz >= 2) for the waits on the
-  // previous stage alone to order all earlier ones
-  if (L.nx < 1 || L.ny < 2 || L.nz < 2 || nzq >= (1 << 15) || lag < 2) return tab;
-  int maxnyq = 1;
-  for (int q = 0; q < 4; ++q) maxnyq = std::max(maxnyq, L.cls[q].nyq);
-  const int lpi = std::min(maxnyq, std::max(1, rows_per_item / L.nx));
-  int ipp[4];
-  for (int q = 0; q < 4; ++q) ipp[q] = (L.cls[q].nyq + lpi - 1) / lpi;
-  struct Entry { int key, s, jz; };
-  std::vector<Entry> es;
-  for (int s = 0; s < 7; ++s) {
-    const int q = wave_class(s), pz = q >> 1;
-    if (ipp[q] == 0) continue;
-    for (int jz = 0; pz + 2 * jz < L.nz; ++jz) es.push_back({pz + 2 * jz + lag * s, s, jz});
-  }
-  std::sort(es.begin(), es.end(), [](const Entry &a, const Entry &b) {
-    return a.key != b.key ? a.key < b.key : a.s < b.s;
-  });
-  int64_t total = 0;
-  for (const Entry &e : es) {
-    tab.push_back(make_int2((e.s << 16) | e.jz, (int)total));
-    total += ipp[wave_class(e.s)];
-  }
-  if (tab.empty() || total >= INT_MAX / 2) return std::vector<int2>();
-  L.wave_ntab = (int)tab.size();
-  L.wave_total = (int)total;
-  L.wave_lpi = lpi;
-  L.wave_nzq = nzq;
-  for (int q = 0; q < 4; ++q) L.wave_ipp[q] = ipp[q];
-  return tab;
-}
-
-template <bool ZERO, bool PRO, bool RES, class VT, class T, class RT>
-void wave_go(const LevelDev &L, const LevelMat<VT> &A, const WaveDev &W, const RT *r, T *x,
-             const T *xc, T *rc, const int *done, cudaStream_t s) {
-  // persistent grid: as many blocks as fit on the GPU at once (the waits do
-  // not depend on it), never more than there are items
-  const size_t smem = (W.uniform > 0 && W.ntab <= kWaveSmemEntries) ? W.ntab * sizeof(int) : 0;
-  static int sms = 0, per_sm[kWaveSmemEntries / 256 + 1] = {};
-  if (!sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    sms = std::max(1, sms);
-  }
-  int &ps = per_sm[(smem / sizeof(int) + 255) / 256];   // by table size in 1 KB steps
-  if (!ps) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_gs_wave<ZERO, PRO, RES, VT, T, RT>,
-                                                  kThreads, (smem / 1024 + 1) * 1024);
-    ps = std::max(1, ps);
-  }
-  const int grid = std::min(sms * ps, W.total);
-  k_gs_wave<ZERO, PRO, RES><<<grid, kThreads, smem, s>>>(A, classes_of(L), W, r, x, xc, rc, done);
-}
-
-template <class T, class RT>
-int launch_gs_wave(const LevelDev &L, int mode, const RT *r, T *x, const T *xc, T *rc,
-                   const int *done, cudaStream_t s) {
-  using VT = typename ValsOf<T>::VT;
-  if (!L.wave_tab || !L.wave_ctr || L.wave_total == 0) return 0;
-  const LevelMat<VT> A = mat_of(L, ValsOf<T>::get(L));
-  WaveDev W;
-  W.tab = L.wave_tab;
-  W.ctr = L.wave_ctr;
-  W.ntab = L.wave_ntab;
-  W.total = L.wave_total;
-  W.lpi = L.wave_lpi;
-  W.nzq = L.wave_nzq;
-  W.nz = L.nz;
-  for (int q = 0; q < 4; ++q) W.ipp[q] = L.wave_ipp[q];
-  W.uniform = L.wave_ipp[0];
-  for (int q = 1; q < 4; ++q)
-    if (L.wave_ipp[q] != W.uniform) W.uniform = 0;
-  switch (mode) {
-    case GS_PLAIN: wave_go<false, false, false>(L, A, W, r, x, xc, rc, done, s); break;
-    case GS_ZERO_GUESS: wave_go<true, false, false>(L, A, W, r, x, xc, rc, done, s); break;
-    case GS_ZERO_GUESS | GS_RESTRICT:
-      wave_go<true, false, true>(L, A, W, r, x, xc, rc, done, s);
-      break;
-    case GS_PROLONG: wave_go<false, true, false>(L, A, W, r, x, xc, rc, done, s); break;
-    default: return 0;
-  }
-  return 1;
-}
-template int launch_gs_wave<double, double>(const LevelDev &, int, const double *, double *,
-                                            const double *, double *, const int *, cudaStream_t);
-template int launch_gs_wave<float, double>(const LevelDev &, int, const double *, float *,
-                                           const float *, float *, const int *, cudaStream_t);
-template int launch_gs_wave<float, float>(const LevelDev &, int, const float *, float *,
-                                          const float *, float *, const int *, cudaStream_t);
-
-int read_wave_fault(unsigned int *fault) {
-  *fault = 0u;
-  cudaError_t e = cudaMemcpyFromSymbol(fault, g_wave_fault, sizeof(*fault));
-  if (e != cudaSuccess) return (int)e;
-  if (*fault) {
-    const unsigned int zero = 0u;
-    e = cudaMemcpyToSymbol(g_wave_fault, &zero, sizeof(zero));
-    if (e != cudaSuccess) return (int)e;
-  }
-  return 0;
-}
-
 int read_check_record(unsigned long long *record) {
   *record = 0ull;
 #ifdef HPCGX_CHECKED
@@ -1752,13 +1618,13 @@ int launch_rank_sum(int nranks, double *const *bufs, int count, cudaStream_t s) 
 
 template int launch_gs_class<double, double>(const LevelDev &, int, int, int, const double *,
                                              double *, const double *, double *, const int *,
-                                             cudaStream_t);
+                                             cudaStream_t, const RzFuse *);
 template int launch_gs_class<float, double>(const LevelDev &, int, int, int, const double *,
                                             float *, const float *, float *, const int *,
-                                            cudaStream_t);
+                                            cudaStream_t, const RzFuse *);
 template int launch_gs_class<float, float>(const LevelDev &, int, int, int, const float *,
                                            float *, const float *, float *, const int *,
-                                           cudaStream_t);
+                                           cudaStream_t, const RzFuse *);
 
 int launch_waxpby(int64_t n, double alpha, const double *x, double beta, const double *y,
                   double *w, const int *done, cudaStream_t s) {
@@ -1768,7 +1634,13 @@ int launch_waxpby(int64_t n, double alpha, const double *x, double beta, const d
 
 int launch_dot(int64_t n, const double *x, const double *y, const Reduce &red, double *out,
                cudaStream_t s) {
-  k_dot<<<vector_blocks(n), kThreads, 0, s>>>(n, x, y, red, out);
+  k_dot<<<vector_blocks(n), kThreads, 0, s>>>(n, x, y, red, FIN_STORE, out, nullptr);
+  return 1;
+}
+
+int launch_dot_finish(int64_t n, const double *x, const double *y, const Reduce &red, int fin,
+                      CgState *st, cudaStream_t s) {
+  k_dot<<<vector_blocks(n), kThreads, 0, s>>>(n, x, y, red, fin, st, &st->done);
   return 1;
 }
 

@@ -15,6 +15,9 @@ struct LevelDev {
   ClassInfo cls[4] = {};
   int lines_per_block[4] = {}, blocks[4] = {}, threads[4] = {};
   int spmv_blocks = 0;        // all four classes in one launch (one line group per block)
+  // FP64 operators derive their columns from the stencil offsets instead of
+  // reading the int32 column arrays (hpcgx_set_stencil_columns)
+  bool stencil_cols = false;
   // z-slab of a sharded problem: a neighbouring rank owns the plane below
   // (zlo) / above (zhi); vectors read by SpMV and Gauss-Seidel then hold one
   // halo plane on each side (indices -nx*ny..-1 and n..n+nx*ny-1)
@@ -26,11 +29,6 @@ struct LevelDev {
   // correction; level 0 uses the caller's vectors)
   double *r64 = nullptr, *x64 = nullptr;
   float *r32 = nullptr, *x32 = nullptr;
-  // one-launch symmetric sweep (k_gs_wave): ticket table and counters
-  int2 *wave_tab = nullptr;   // wave_ntab entries
-  int *wave_ctr = nullptr;    // 7 * wave_nzq + 3 ints, zero between launches
-  int wave_ntab = 0, wave_total = 0, wave_lpi = 0, wave_nzq = 0;
-  int wave_ipp[4] = {};
 };
 
 // Device-side state of a CG solve (scalars never leave the GPU except the
@@ -74,7 +72,31 @@ enum GsMode : int {
   GS_ZERO_GUESS = 1,
   GS_RESTRICT = 2,
   GS_PROLONG = 4,
-  GS_SYM3 = 8
+  GS_SYM3 = 8,
+  // GS_DOT: one of the four launches that write the finest level's final
+  // correction z (the post-smoother's class 3 forward+backward and backward
+  // classes 2, 1, 0) also takes CG's r.z and, for the flexible solver,
+  // z.Ap_{k-1} over the rows it finalises (mixed V-cycle only)
+  GS_DOT = 16,
+  // internal to the kernels: the FP64 sweeps derive their columns from the
+  // stencil offsets (LevelDev::stencil_cols)
+  GS_STENCIL = 32,
+  // internal to the kernels: the mixed sweeps' x gathers take the aligned
+  // pair of a row's three x-neighbours on a line in one 8-byte load
+  GS_VEC = 64
+};
+
+// The r.z reduction of src/CG.cpp:109-112 spread over the four GS_DOT
+// launches: each reduces its rows deterministically; launches 0-2 store their
+// totals in part, launch 3 adds the four totals in launch order and runs
+// CG's beta step (FIN_CG_RZ) -- or defers it on a sharded problem.
+struct RzFuse {
+  Reduce red;
+  double *part = nullptr;     // 3 x 2 totals
+  CgState *st = nullptr;
+  const double *Ap = nullptr; // A p of the previous iteration (flexible solver)
+  int slot = 0;               // 0..3
+  int flex = 0;
 };
 
 // Layout / set-up ---------------------------------------------------------
@@ -99,13 +121,18 @@ int launch_spmv32(const LevelDev &L, const float *x, float *y, cudaStream_t s);
 // vectors) or float (BF16 values, FP32 vectors); RT is the right-hand side type.
 template <class T, class RT>
 int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                     const T *xc, T *rc, const int *done, cudaStream_t s);
+                     const T *xc, T *rc, const int *done, cudaStream_t s,
+                     const RzFuse *rz = nullptr);
+
 
 // Vectors -----------------------------------------------------------------
 int launch_waxpby(int64_t n, double alpha, const double *x, double beta, const double *y,
                    double *w, const int *done, cudaStream_t s);
 int launch_dot(int64_t n, const double *x, const double *y, const Reduce &red, double *out,
                 cudaStream_t s);
+// x.y followed by the CG scalar step `fin` (skipped once st->done is set).
+int launch_dot_finish(int64_t n, const double *x, const double *y, const Reduce &red, int fin,
+                      CgState *st, cudaStream_t s);
 int launch_absmax_diff(int64_t n, const double *a, const double *b, const Reduce &red,
                         double *out, cudaStream_t s);
 int launch_restriction(int64_t nc, const LevelDev &F, const double *rf, const double *Axf,
@@ -140,18 +167,6 @@ int launch_restrict_residual(const LevelDev &F, int64_t nc, const RT *rf, const 
 template <class T>
 int launch_prolong(const LevelDev &F, int64_t nc, const T *xc, T *xf, const int *done,
                    cudaStream_t s);
-// One symmetric Gauss-Seidel sweep of a level in one launch (k_gs_wave), the
-// same result as its seven class launches.  mode: GS_PLAIN, or GS_ZERO_GUESS
-// (optionally | GS_RESTRICT into rc), or GS_PROLONG (adding xc first).
-// wave_plan fills the wave_* fields of L but the two device pointers and
-// returns the ticket table to upload (items of about rows_per_item rows,
-// stage lag `lag` planes); an empty table disables the launch.
-std::vector<int2> wave_plan(LevelDev &L, int lag, int rows_per_item);
-template <class T, class RT>
-int launch_gs_wave(const LevelDev &L, int mode, const RT *r, T *x, const T *xc, T *rc,
-                   const int *done, cudaStream_t s);
-// 1 if a one-launch sweep gave up waiting since the last call (then cleared)
-int read_wave_fault(unsigned int *fault);
 template <class ZT>
 int launch_cg_rz(int64_t n, const double *r, const ZT *z, const double *Ap, const Reduce &red,
                   CgState *st, cudaStream_t s);

@@ -10,6 +10,7 @@
 // (a file-scope __device__ array, loaded with the module), so a call
 // allocates nothing; the caller passes the input vectors and the device
 // location of the result.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -35,8 +36,51 @@ static_assert(HPCGX_DOT_NOALLOC_MAX_N % kPerBlock == 0, "limit must be a whole n
 // library, held until the process exits.
 static __device__ __align__(256) double g_dot_scratch[kMaxPartials + 32];
 
-void *g_scratch_addr[kMaxDevices] = {};
+// The address of g_dot_scratch, cached per device together with the unique
+// id of the context it was resolved in: after cudaDeviceReset (or any other
+// teardown of the primary context) the module is loaded again and the array
+// may move, so a cached address is only reused in the same context.
+struct ScratchCache {
+  unsigned long long ctx_id;
+  void *addr;
+};
+ScratchCache g_scratch[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
+
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points, so
+// that the library needs no link against libcuda.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// *id = 0 when the thread has no current context yet (the runtime creates the
+// primary context lazily, e.g. in cudaGetSymbolAddress).
+int current_context_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void *f1 = nullptr, *f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1, q2;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f1, 12000, cudaEnableDefault, &q1) !=
+            cudaSuccess ||
+        cudaGetDriverEntryPointByVersion("cuCtxGetId", &f2, 12000, cudaEnableDefault, &q2) !=
+            cudaSuccess ||
+        q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2) {
+      cudaGetLastError();
+      return hpcgx::set_error(HPCGX_ECUDA,
+                              "hpcgx_dot_noalloc: driver entry points cuCtxGetCurrent/cuCtxGetId "
+                              "unavailable");
+    }
+    get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+    get_id = reinterpret_cast<CtxGetIdFn>(f2);
+  }
+  CUcontext ctx = nullptr;
+  *id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS)
+    return hpcgx::set_error(HPCGX_ECUDA, "hpcgx_dot_noalloc: cuCtxGetCurrent failed");
+  if (ctx && get_id(ctx, id) != CUDA_SUCCESS)
+    return hpcgx::set_error(HPCGX_ECUDA, "hpcgx_dot_noalloc: cuCtxGetId failed");
+  return HPCGX_OK;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -45,8 +89,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Each block reduces its 2048 elements to one partial; the last block to
-// arrive adds the partials in block order (so the result does not depend on
-// which block finishes last), writes the result and re-arms the counter.
+// arrive adds the partials in a fixed order that depends only on the grid
+// size (strided per-thread sums, then a warp shuffle tree, then the warps in
+// order), so the result does not depend on which block finishes last; it
+// writes the result and re-arms the counter.
 __global__ void __launch_bounds__(kThreads)
 k_dot_noalloc(int64_t n, const double *__restrict__ x, const double *__restrict__ y,
               double *partials, unsigned int *counter, double *result) {
@@ -88,20 +134,31 @@ k_dot_noalloc(int64_t n, const double *__restrict__ x, const double *__restrict_
 }
 
 // Device address of g_dot_scratch on the current device, resolved once per
-// device.  In host code the symbol name is only a host-side handle; the
-// kernel must be given this address instead.
+// device and context.  In host code the symbol name is only a host-side
+// handle; the kernel must be given this address instead.
 int scratch_for_device(int dev, double **out) {
   if (dev < 0 || dev >= kMaxDevices)
     return hpcgx::set_error(HPCGX_EINVAL, "hpcgx_dot_noalloc: device index out of range");
+  unsigned long long ctx_id = 0;
+  int rc = current_context_id(&ctx_id);
+  if (rc != HPCGX_OK) return rc;
   std::lock_guard<std::mutex> lock(g_scratch_mutex);
-  if (!g_scratch_addr[dev]) {
+  ScratchCache &c = g_scratch[dev];
+  if (!c.addr || ctx_id == 0 || c.ctx_id != ctx_id) {
     void *ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_dot_scratch);
-    if (e != cudaSuccess || !ptr)
+    if (e != cudaSuccess || !ptr) {
+      cudaGetLastError();
       return hpcgx::set_error(HPCGX_ECUDA, "hpcgx_dot_noalloc: cudaGetSymbolAddress failed");
-    g_scratch_addr[dev] = ptr;
+    }
+    if (ctx_id == 0) {   // the lookup above created the context
+      rc = current_context_id(&ctx_id);
+      if (rc != HPCGX_OK) return rc;
+    }
+    c.addr = ptr;
+    c.ctx_id = ctx_id;
   }
-  *out = static_cast<double *>(g_scratch_addr[dev]);
+  *out = static_cast<double *>(c.addr);
   return HPCGX_OK;
 }
 

@@ -12,6 +12,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <memory>
 #include <chrono>
 #include <cmath>
@@ -26,6 +27,7 @@
 #include <vector>
 
 #include "../../include/hpcgx.h"
+#include "general.cuh"
 #include "kernels.cuh"
 
 using namespace hpcgx;
@@ -128,6 +130,9 @@ static int env_int(const char *name, int dflt) {
 struct hpcgx_problem {
   int device = 0;
   int nlev = 0;
+  // a general-pattern problem (hpcgx_create_general): the operators run on
+  // this instead of the stencil levels below, which stay empty
+  GeneralProblem *gen = nullptr;
   LevelDev L[kMaxLevels];
   cudaStream_t stream = nullptr;      // stream in use
   cudaStream_t own_stream = nullptr;  // stream created with the problem
@@ -140,12 +145,16 @@ struct hpcgx_problem {
   double *tmp = nullptr;      // staging for host diagonals
   double *stage[3] = {};      // staging of the host-buffer operators (allocated on first use)
   double *result = nullptr;   // device scalars of standalone reductions
+  double *rz_part = nullptr;  // totals of the first three GS_DOT launches (3 x 2)
   CgState *st = nullptr;
   Reduce red;
   // graphs of one CG iteration
   cudaGraphExec_t graph[G_COUNT] = {};
   int graph_kernels[G_COUNT] = {};
   int graph_probe[G_COUNT] = {};
+  // algorithmic bytes of one iteration of each graph (this implementation's
+  // byte model, summed over its launches while the graph is captured)
+  double graph_bytes[G_COUNT] = {};
   cudaEvent_t phase[G_COUNT][5] = {};
   // capture bookkeeping
   bool capturing = false;
@@ -172,18 +181,6 @@ struct hpcgx_problem {
   double *gsum = nullptr;            // this rank's deferred reduction totals
   double *hstage[kMaxLevels] = {};   // haloed FP64 staging of operator inputs
   bool sharded() const { return nranks > 1 || nccl != nullptr || comm_halo != nullptr; }
-  // symmetric sweeps in one launch (k_gs_wave) instead of seven class launches
-  bool wave = false;
-  bool use_wave(int l) const { return wave && L[l].wave_tab != nullptr; }
-  // a one-launch sweep that gave up waiting is reported once the stream is idle
-  int wave_check() {
-    if (!wave) return HPCGX_OK;
-    unsigned int f = 0u;
-    const int e = read_wave_fault(&f);
-    if (e != 0) return cuda_fail((cudaError_t)e);
-    if (f) return fail(HPCGX_ETIMEOUT, "a one-launch Gauss-Seidel sweep gave up waiting for a stage");
-    return HPCGX_OK;
-  }
 
   ~hpcgx_problem();
   int alloc(void **ptr, size_t n) {
@@ -243,6 +240,7 @@ struct hpcgx_problem {
   // (once) if one of them is armed and a graph is being captured.
   template <class F>
   int probed(int kinds, double bytes_model, F &&launch) {
+    if (capturing) graph_bytes[capture_kind] += bytes_model;
     const int armed = capturing ? (kinds & probe) : 0;
     if (armed) {
       if (pool_next >= event_pool.size()) return fail(HPCGX_ESTATE, "probe event pool exhausted");
@@ -266,49 +264,38 @@ struct hpcgx_problem {
   // ---- multigrid
   template <class T, class RT0>
   int gs_launch(int l, int q, int backward, int mode, const void *r, T *x, const T *xc, T *rc,
-                const int *done) {
+                const int *done, const RzFuse *rz = nullptr) {
     const bool mixed = std::is_same<T, float>::value;
+    const int sweep = mode & ~GS_DOT;
     int kinds = 0;
     if (l == 0) {
       kinds |= HPCGX_PROBE_GS_FINE;
-      if (mode == GS_PLAIN && backward) kinds |= HPCGX_PROBE_GS_FINE_BWD;
+      if (sweep == GS_PLAIN && backward) kinds |= HPCGX_PROBE_GS_FINE_BWD;
     }
-    return probed(kinds, (kinds & probe) ? gs_bytes(l, q, mode, mixed) : 0.0, [&]() {
-      if (l == 0)
-        return launch_gs_class<T, RT0>(L[l], q, backward, mode, static_cast<const RT0 *>(r), x,
-                                       xc, rc, done, stream);
-      return launch_gs_class<T, T>(L[l], q, backward, mode, static_cast<const T *>(r), x, xc,
-                                   rc, done, stream);
-    });
-  }
-
-  // One symmetric sweep of level l in one launch; probed as the finest
-  // level's Gauss-Seidel with the bytes of its seven class steps.
-  template <class T, class RT0>
-  int wave_launch(int l, int mode, const void *r, T *x, const T *xc, T *rc, const int *done) {
-    const bool mixed = std::is_same<T, float>::value;
-    const int kinds = l == 0 ? HPCGX_PROBE_GS_FINE : 0;
     double bytes = 0.0;
-    if (kinds & probe) {
-      const int m0 = mode & GS_ZERO_GUESS;
-      for (int q = 0; q < 3; ++q)
-        bytes += gs_bytes(l, q, (q == 0 && (mode & GS_PROLONG)) ? GS_PROLONG : m0, mixed);
-      bytes += gs_bytes(l, 3, GS_SYM3 | m0, mixed);
-      for (int q = 2; q >= 0; --q)
-        bytes += gs_bytes(l, q, (q == 0 && (mode & GS_RESTRICT)) ? GS_RESTRICT : GS_PLAIN, mixed);
+    if ((kinds & probe) || capturing) {
+      bytes = gs_bytes(l, q, sweep, mixed);
+      // GS_DOT reads A p of the previous iteration for the rows it finalises
+      // (all but the first iteration; counted for every one)
+      if ((mode & GS_DOT) && rz && rz->flex)
+        bytes += 8.0 * (double)(L[l].ccount[2 * q] + L[l].ccount[2 * q + 1]);
     }
     return probed(kinds, bytes, [&]() {
       if (l == 0)
-        return launch_gs_wave<T, RT0>(L[l], mode, static_cast<const RT0 *>(r), x, xc, rc, done,
-                                      stream);
-      return launch_gs_wave<T, T>(L[l], mode, static_cast<const T *>(r), x, xc, rc, done, stream);
+        return launch_gs_class<T, RT0>(L[l], q, backward, mode, static_cast<const RT0 *>(r), x,
+                                       xc, rc, done, stream, rz);
+      return launch_gs_class<T, T>(L[l], q, backward, mode, static_cast<const T *>(r), x, xc,
+                                   rc, done, stream, rz);
     });
   }
 
   // One V-cycle (src/ComputeMG_ref.cpp:39-63) with all levels fused as
-  // described in kernels.cu.  r0 / x0 are the finest level's vectors.
+  // described in kernels.cu.  r0 / x0 are the finest level's vectors.  With
+  // rz, the four launches that finalise x0 (the finest post-smoother's class 3
+  // forward+backward and backward classes 2, 1, 0) also take CG's r.z
+  // (GS_DOT, slots 0..3); the caller checked that they can (rz_fusable).
   template <class T, class RT0>
-  int vcycle(const RT0 *r0, T *x0, const int *done) {
+  int vcycle(const RT0 *r0, T *x0, const int *done, const RzFuse *rz = nullptr) {
     const void *rl[kMaxLevels];
     T *xl[kMaxLevels];
     for (int l = 0; l < nlev; ++l) {
@@ -316,15 +303,9 @@ struct hpcgx_problem {
       xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
     }
     // Each symmetric sweep: forward classes 0..2, class 3 forward+backward in
-    // one launch (GS_SYM3), backward classes 2..0 -- 7 launches, or one
-    // k_gs_wave launch doing the same seven steps.
+    // one launch (GS_SYM3), backward classes 2..0 -- 7 launches.
     // descend: pre-smooth (zero initial guess) and restrict
     for (int l = 0; l + 1 < nlev; ++l) {
-      if (use_wave(l)) {
-        TRY((wave_launch<T, RT0>(l, GS_ZERO_GUESS | GS_RESTRICT, rl[l], xl[l], nullptr,
-                                 lvl_r(L[l + 1], (T *)nullptr), done)));
-        continue;
-      }
       for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr, done)));
       TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[l], xl[l], nullptr, nullptr,
@@ -335,39 +316,52 @@ struct hpcgx_problem {
     }
     // coarsest level: one symmetric sweep from zero
     const int c = nlev - 1;
-    if (use_wave(c)) {
-      TRY((wave_launch<T, RT0>(c, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
-    } else {
-      for (int q = 0; q < 3; ++q)
-        TRY((gs_launch<T, RT0>(c, q, 0, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
-      TRY((gs_launch<T, RT0>(c, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr,
-                             done)));
-      for (int q = 2; q >= 0; --q)
-        TRY((gs_launch<T, RT0>(c, q, 1, GS_PLAIN, rl[c], xl[c], nullptr, nullptr, done)));
-    }
+    for (int q = 0; q < 3; ++q)
+      TRY((gs_launch<T, RT0>(c, q, 0, GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr, done)));
+    TRY((gs_launch<T, RT0>(c, 3, 0, GS_SYM3 | GS_ZERO_GUESS, rl[c], xl[c], nullptr, nullptr,
+                           done)));
+    for (int q = 2; q >= 0; --q)
+      TRY((gs_launch<T, RT0>(c, q, 1, GS_PLAIN, rl[c], xl[c], nullptr, nullptr, done)));
     // ascend: prolongate and post-smooth
     for (int l = nlev - 2; l >= 0; --l) {
-      if (use_wave(l)) {
-        TRY((wave_launch<T, RT0>(l, GS_PROLONG, rl[l], xl[l], lvl_x(L[l + 1], (T *)nullptr),
-                                 nullptr, done)));
-        continue;
-      }
       for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, q == 0 ? GS_PROLONG : GS_PLAIN, rl[l], xl[l],
                                lvl_x(L[l + 1], (T *)nullptr), nullptr, done)));
-      TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3, rl[l], xl[l], nullptr, nullptr, done)));
+      RzFuse f[4];
+      const bool dot = rz && l == 0;
+      for (int i = 0; dot && i < 4; ++i) {
+        f[i] = *rz;
+        f[i].slot = i;
+      }
+      TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3 | (dot ? GS_DOT : 0), rl[l], xl[l], nullptr,
+                             nullptr, done, dot ? &f[0] : nullptr)));
       for (int q = 2; q >= 0; --q)
-        TRY((gs_launch<T, RT0>(l, q, 1, GS_PLAIN, rl[l], xl[l], nullptr, nullptr, done)));
+        TRY((gs_launch<T, RT0>(l, q, 1, GS_PLAIN | (dot ? GS_DOT : 0), rl[l], xl[l], nullptr,
+                               nullptr, done, dot ? &f[3 - q] : nullptr)));
     }
     return HPCGX_OK;
   }
 
+  // The mixed solver's r.z rides on its V-cycle's last four launches when the
+  // V-cycle has a coarse level (so that those launches are the finest
+  // post-smoother's); HPCGX_FUSE_RZ=0 keeps k_cg_rz.  The sharded solver
+  // defers the totals to the sum over the ranks, as k_cg_rz's.
+  bool rz_fusable() const {
+    static const bool on = env_int("HPCGX_FUSE_RZ", 1) != 0;
+    return on && nlev >= 2 && rz_part;
+  }
+  RzFuse rz_fuse(bool defer = false) const {
+    RzFuse f;
+    f.red = defer ? deferred() : red;
+    f.part = rz_part;
+    f.st = st;
+    f.Ap = Ap;
+    f.flex = 1;
+    return f;
+  }
+
   template <class T, class RT>
   int symgs(int l, const RT *r, T *x) {
-    if (use_wave(l)) {
-      note(launch_gs_wave<T, RT>(L[l], GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
-      return HPCGX_OK;
-    }
     for (int q = 0; q < 3; ++q)
       note(launch_gs_class<T, RT>(L[l], q, 0, GS_PLAIN, r, x, nullptr, nullptr, nullptr, stream));
     note(launch_gs_class<T, RT>(L[l], 3, 0, GS_SYM3, r, x, nullptr, nullptr, nullptr, stream));
@@ -414,23 +408,40 @@ struct hpcgx_problem {
       note(launch_copy_z(n, r, z, st, stream));
     } else if (kind == G_FP64_PREC) {
       TRY((vcycle<double, double>(r, z, done)));
+    } else if (rz_fusable()) {
+      const RzFuse f = rz_fuse();
+      TRY((vcycle<float, double>(r, z32, done, &f)));
     } else {
       TRY((vcycle<float, double>(r, z32, done)));
     }
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][1], stream, cudaEventRecordExternal));
+    // vector kernels, bytes per row: r.z reads r, z (and Ap); p = z + beta p
+    // reads z and p and writes p; x += alpha p, r -= alpha Ap reads p, Ap and
+    // reads and writes x and r
+    auto vec_bytes = [&](double per_row) {
+      if (capturing) graph_bytes[kind] += per_row * (double)n;
+    };
+    if (kind == G_FP64_NOPREC) vec_bytes(16.0);
     if (kind == G_MIXED) {
-      note(launch_cg_rz<float>(n, r, z32, Ap, red, st, stream));
+      // r.z and z.Ap_{k-1} (src/CG.cpp:109-112): taken by the V-cycle's last
+      // launches when they can, else here
+      if (!rz_fusable()) {
+        note(launch_cg_rz<float>(n, r, z32, Ap, red, st, stream));
+        vec_bytes(20.0);
+      }
       note(launch_cg_p<float>(n, z32, p, st, stream));
+      vec_bytes(20.0);
     } else {
       note(launch_cg_rz<double>(n, r, z, nullptr, red, st, stream));
       note(launch_cg_p<double>(n, z, p, st, stream));
+      vec_bytes(16.0 + 24.0);
     }
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][2], stream, cudaEventRecordExternal));
     // The mixed solver's FP64 SpMV derives its columns from the stencil
     // offsets; the plain FP64 solver reads the int32 column arrays.
-    const bool implicit_cols = kind == G_MIXED;
+    const bool implicit_cols = kind == G_MIXED || L[0].stencil_cols;
     double spmv_bytes = 0.0;
-    if (probe & HPCGX_PROBE_SPMV_FINE) {
+    if ((probe & HPCGX_PROBE_SPMV_FINE) || capturing) {
       // 12 B (8 B without column reads) per real nonzero, x and y once; the
       // fused p.Ap reads nothing extra
       int64_t nnz = 0;
@@ -449,6 +460,7 @@ struct hpcgx_problem {
     }));
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][3], stream, cudaEventRecordExternal));
     note(launch_cg_xr(n, p, Ap, x, r, red, st, stream));
+    vec_bytes(48.0);
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][4], stream, cudaEventRecordExternal));
     return HPCGX_OK;
   }
@@ -477,6 +489,7 @@ struct hpcgx_problem {
     }
     cudaGraph_t g = nullptr;
     const int64_t before = launches;
+    graph_bytes[kind] = 0.0;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     capturing = true;
     capture_kind = kind;
@@ -555,9 +568,13 @@ struct hpcgx_problem {
       }
       if (h.done) break;
     }
+    if (launched == 0) {
+      // max_iter == 0: no iteration ran, but the initial residual norm is
+      // still a result (src/CG.cpp:89-96 sets normr and normr0 before the loop)
+      CK(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    }
     if (xu != x) CK(cudaMemcpyAsync(xu, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     CK(cudaStreamSynchronize(stream));
-    TRY(wave_check());
     if (niters) *niters = h.niters;
     if (normr) *normr = h.normr;
     if (normr0) *normr0 = h.normr0;
@@ -618,14 +635,29 @@ struct hpcgx_problem {
   // rc: the last backward class forms the restricted residual (GS_RESTRICT).
   template <class T, class RT>
   void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done,
-                   const T *xc = nullptr, T *rc = nullptr) {
+                   const T *xc = nullptr, T *rc = nullptr, const RzFuse *rz = nullptr) {
     const int m0 = zero ? GS_ZERO_GUESS : GS_PLAIN;
-    if (use_wave(l)) {
-      const int m = xc ? GS_PROLONG : m0 | (rc ? GS_RESTRICT : 0);
-      add(pl, [=]() {
-        note(launch_gs_wave<T, RT>(L[l], m, r, x, xc, rc, done, stream));
-        return HPCGX_OK;
-      });
+    if (rz) {   // the finest post-smoother of the mixed solver: GS_DOT, slots 0..3
+      for (int q = 0; q < 3; ++q) {
+        const int m = (q == 0 && xc) ? GS_PROLONG : m0;
+        add(pl, [=]() {
+          note(launch_gs_class<T, RT>(L[l], q, 0, m, r, x, xc, nullptr, done, stream));
+          return HPCGX_OK;
+        });
+      }
+      for (int i = 0; i < 4; ++i) {
+        RzFuse f = *rz;
+        f.slot = i;
+        const int q = i == 0 ? 3 : 3 - i;
+        const int m = (i == 0 ? GS_SYM3 : GS_PLAIN) | GS_DOT;
+        add(pl, [=]() {
+          const int k = launch_gs_class<T, RT>(L[l], q, i == 0 ? 0 : 1, m, r, x, nullptr, nullptr,
+                                               done, stream, &f);
+          if (!k) return fail(HPCGX_ESTATE, "the fused r.z sweep is not available here");
+          note(k);
+          return HPCGX_OK;
+        });
+      }
       return;
     }
     for (int q = 0; q < 3; ++q) {
@@ -659,7 +691,7 @@ struct hpcgx_problem {
   // correction (which the fused prolongation then skips).  x0 must be a
   // haloed vector.
   template <class T, class RT0>
-  void plan_vcycle(Plan &pl, const RT0 *r0, T *x0, const int *done) {
+  void plan_vcycle(Plan &pl, const RT0 *r0, T *x0, const int *done, const RzFuse *rz = nullptr) {
     T *xl[kMaxLevels];
     for (int l = 0; l < nlev; ++l) xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
     auto rl = [&](int l) { return lvl_r(L[l], (T *)nullptr); };
@@ -707,7 +739,7 @@ struct hpcgx_problem {
       });
       add_halo(pl, l, x, sizeof(T));
       if (l == 0)
-        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc);
+        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc, nullptr, rz);
       else
         plan_sweeps<T, T>(pl, l, rl(l), x, false, done, xc);
     }
@@ -784,17 +816,23 @@ struct hpcgx_problem {
       });
     else if (kind == G_FP64_PREC)
       plan_vcycle<double, double>(pl, r, z, done);
-    else
-      plan_vcycle<float, double>(pl, r, z32, done);
     const bool mixed = kind == G_MIXED;
-    add(pl, [=]() {
-      if (mixed) {
-        note(launch_cg_rz<float>(n, r, z32, Ap, deferred(), st, stream));
-      } else {
-        note(launch_cg_rz<double>(n, r, z, nullptr, deferred(), st, stream));
-      }
-      return HPCGX_OK;
-    });
+    // the mixed solver's r.z inside its V-cycle (as the graph solver's), else
+    // a separate reduction; either way the totals are deferred to the sum
+    const bool fused = mixed && rz_fusable();
+    if (mixed) {
+      const RzFuse f = rz_fuse(true);
+      plan_vcycle<float, double>(pl, r, z32, done, fused ? &f : nullptr);
+    }
+    if (!fused)
+      add(pl, [=]() {
+        if (mixed) {
+          note(launch_cg_rz<float>(n, r, z32, Ap, deferred(), st, stream));
+        } else {
+          note(launch_cg_rz<double>(n, r, z, nullptr, deferred(), st, stream));
+        }
+        return HPCGX_OK;
+      });
     add_sum(pl, FIN_CG_RZ, mixed ? 2 : 1);
     add(pl, [=]() {
       if (mixed)
@@ -843,8 +881,10 @@ hpcgx_problem::~hpcgx_problem() {
   for (double *ptr : stage) cudaFree(ptr);
   for (void *ptr : halo_bases) cudaFree(ptr);
   for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)Ap, (void *)tmp, (void *)result,
-                    (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter})
+                    (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter,
+                    (void *)rz_part})
     cudaFree(ptr);
+  if (gen) general_destroy(gen);
   if (own_stream) cudaStreamDestroy(own_stream);
 }
 
@@ -860,6 +900,18 @@ namespace {
 int check_level(hpcgx_problem *p, int level) {
   if (level < 0 || level >= p->nlev)
     return fail(HPCGX_EINVAL, "level " + std::to_string(level) + " out of range");
+  return HPCGX_OK;
+}
+
+// Operators that exist only for the 27-point stencil layout.
+int stencil_only(hpcgx_problem *p, const char *what) {
+  if (p->gen)
+    return fail(HPCGX_ESTATE, std::string(what) + " is not available on a general-pattern problem");
+  return HPCGX_OK;
+}
+
+int general_ready_or_fail(hpcgx_problem *p) {
+  if (!general_ready(p->gen)) return fail(HPCGX_ESTATE, "not every level is loaded");
   return HPCGX_OK;
 }
 
@@ -989,6 +1041,9 @@ struct NcclApi {
   ncclResult_t (*GroupStart)() = nullptr;
   ncclResult_t (*GroupEnd)() = nullptr;
   const char *(*GetErrorString)(ncclResult_t) = nullptr;
+  ncclResult_t (*CommInitRankConfig)(ncclComm_t *, int, ncclUniqueId, int, ncclConfig_t *) = nullptr;
+  ncclResult_t (*CommGetAsyncError)(ncclComm_t, ncclResult_t *) = nullptr;
+  ncclResult_t (*CommAbort)(ncclComm_t) = nullptr;
 };
 
 static NcclApi *nccl_api() {
@@ -1008,27 +1063,84 @@ static NcclApi *nccl_api() {
     api.GroupStart = (decltype(api.GroupStart))dlsym(h, "ncclGroupStart");
     api.GroupEnd = (decltype(api.GroupEnd))dlsym(h, "ncclGroupEnd");
     api.GetErrorString = (decltype(api.GetErrorString))dlsym(h, "ncclGetErrorString");
+    api.CommInitRankConfig =
+        (decltype(api.CommInitRankConfig))dlsym(h, "ncclCommInitRankConfig");
+    api.CommGetAsyncError = (decltype(api.CommGetAsyncError))dlsym(h, "ncclCommGetAsyncError");
+    api.CommAbort = (decltype(api.CommAbort))dlsym(h, "ncclCommAbort");
     ok = api.GetUniqueId && api.CommInitRank && api.CommDestroy && api.Send && api.Recv &&
-         api.AllReduce && api.GroupStart && api.GroupEnd && api.GetErrorString;
+         api.AllReduce && api.GroupStart && api.GroupEnd && api.GetErrorString &&
+         api.CommInitRankConfig && api.CommGetAsyncError && api.CommAbort;
   });
   return ok ? &api : nullptr;
 }
 
-#define NCCLCK(call)                                                                  \
-  do {                                                                                \
-    ncclResult_t r_ = (call);                                                         \
-    if (r_ != ncclSuccess)                                                            \
-      return fail(HPCGX_ECOMM, std::string(#call) + ": " + nccl_api()->GetErrorString(r_)); \
-  } while (0)
-
+// The communicator is non-blocking (ncclConfig_t::blocking = 0): a call may
+// return ncclInProgress, and the communicator's state is then polled with
+// ncclCommGetAsyncError until it settles -- for at most HPCGX_WAIT_TIMEOUT_S,
+// after which the communicator is aborted (ncclCommAbort, which also stops
+// its kernels) and the call returns HPCGX_ETIMEOUT instead of blocking
+// behind a peer that has failed.  The reference aborts on a failed exchange
+// too (src/ExchangeHalo.cpp:102-104).
 struct NcclLink {
   ncclComm_t comm = nullptr;
+  bool aborted = false;
 };
 
+double wait_limit_s() {
+  static const double limit = [] {
+    const char *e = std::getenv("HPCGX_WAIT_TIMEOUT_S");
+    const double v = e ? std::atof(e) : 0.0;
+    return v > 0.0 ? v : 600.0;
+  }();
+  return limit;
+}
+
+void nccl_abort(NcclLink *link) {
+  if (link->comm && !link->aborted && nccl_api()) nccl_api()->CommAbort(link->comm);
+  link->aborted = true;
+}
+
 void nccl_release(NcclLink *link) {
-  if (link->comm && nccl_api()) nccl_api()->CommDestroy(link->comm);
+  if (link->comm && !link->aborted && nccl_api()) nccl_api()->CommDestroy(link->comm);
   delete link;
 }
+
+// Waits (bounded) until the communicator has settled after a call that
+// returned r; aborts it on a timeout or an error.
+// Fault injection for tests, on the host: HPCGX_FAULT_NCCL_STALL=k makes the
+// first k settles of the process see a communicator that never leaves
+// ncclInProgress, as behind a peer that has died (no GPU fault involved).
+bool nccl_fake_stall() {
+  static std::atomic<int> left{env_int("HPCGX_FAULT_NCCL_STALL", 0)};
+  return left.fetch_sub(1) > 0;
+}
+
+int nccl_settle(NcclLink *link, ncclResult_t r, const char *what) {
+  NcclApi *api = nccl_api();
+  const double t0 = now_s();
+  const bool stall = (r == ncclSuccess || r == ncclInProgress) && nccl_fake_stall();
+  if (stall) r = ncclInProgress;
+  for (int polls = 0; r == ncclInProgress; ++polls) {
+    if (api->CommGetAsyncError(link->comm, &r) != ncclSuccess) r = ncclInternalError;
+    if (stall && r == ncclSuccess) r = ncclInProgress;
+    if (r != ncclInProgress) break;
+    if (now_s() - t0 > wait_limit_s()) {
+      nccl_abort(link);
+      return fail(HPCGX_ETIMEOUT, std::string(what) +
+                                      ": the NCCL communicator did not settle within "
+                                      "HPCGX_WAIT_TIMEOUT_S; it was aborted");
+    }
+    if (polls > 2000) std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  if (r != ncclSuccess) {
+    nccl_abort(link);
+    return fail(HPCGX_ECOMM, std::string(what) + ": " + api->GetErrorString(r) +
+                                 " (the communicator was aborted)");
+  }
+  return HPCGX_OK;
+}
+
+#define NCCLCK(link, call) TRY(nccl_settle((link), (call), #call))
 
 namespace {
 
@@ -1042,17 +1154,23 @@ int nccl_halo(hpcgx_problem *p, int l, void *v, int esize) {
   const size_t plane = (size_t)A.nx * A.ny;
   const ncclDataType_t t = esize == 8 ? ncclFloat64 : ncclFloat32;
   char *b = static_cast<char *>(v);
-  ncclComm_t c = p->nccl->comm;
-  NCCLCK(api->GroupStart());
-  if (A.zlo) {
-    NCCLCK(api->Send(b, plane, t, p->rank - 1, c, p->stream));
-    NCCLCK(api->Recv(b - plane * esize, plane, t, p->rank - 1, c, p->stream));
+  NcclLink *link = p->nccl;
+  ncclComm_t c = link->comm;
+  // inside a group the calls only record the operations; GroupEnd issues them
+  ncclResult_t r = api->GroupStart();
+  if (A.zlo && (r == ncclSuccess || r == ncclInProgress)) {
+    r = api->Send(b, plane, t, p->rank - 1, c, p->stream);
+    if (r == ncclSuccess || r == ncclInProgress)
+      r = api->Recv(b - plane * esize, plane, t, p->rank - 1, c, p->stream);
   }
-  if (A.zhi) {
-    NCCLCK(api->Send(b + (A.n - (int64_t)plane) * esize, plane, t, p->rank + 1, c, p->stream));
-    NCCLCK(api->Recv(b + A.n * esize, plane, t, p->rank + 1, c, p->stream));
+  if (A.zhi && (r == ncclSuccess || r == ncclInProgress)) {
+    r = api->Send(b + (A.n - (int64_t)plane) * esize, plane, t, p->rank + 1, c, p->stream);
+    if (r == ncclSuccess || r == ncclInProgress)
+      r = api->Recv(b + A.n * esize, plane, t, p->rank + 1, c, p->stream);
   }
-  NCCLCK(api->GroupEnd());
+  const ncclResult_t e = api->GroupEnd();
+  if (r == ncclSuccess || r == ncclInProgress) r = e;
+  NCCLCK(link, r);
   return HPCGX_OK;
 }
 
@@ -1076,6 +1194,9 @@ int callback_halo(hpcgx_problem *p, int l, void *v, int esize) {
 // attached backend (NCCL or the caller's functions).  Without one (one rank)
 // both are no-ops.
 int run_plan(hpcgx_problem *p, Plan &pl) {
+  if (p->nccl && p->nccl->aborted)
+    return fail(HPCGX_ESTATE, "the NCCL communicator was aborted after a timeout or an error; "
+                              "attach a new one (hpcgx_attach_nccl)");
   for (Step &s : pl) {
     if (s.kind == STEP_LAUNCH) {
       TRY(s.launch());
@@ -1084,8 +1205,8 @@ int run_plan(hpcgx_problem *p, Plan &pl) {
       else if (p->comm_halo) TRY(callback_halo(p, s.level, s.vec, s.esize));
     } else {
       if (p->nccl)
-        NCCLCK(nccl_api()->AllReduce(p->gsum, p->gsum, s.nv, ncclFloat64, ncclSum, p->nccl->comm,
-                                     p->stream));
+        NCCLCK(p->nccl, nccl_api()->AllReduce(p->gsum, p->gsum, s.nv, ncclFloat64, ncclSum,
+                                              p->nccl->comm, p->stream));
       else if (p->comm_sum &&
                p->comm_sum(p->comm_ctx, p->gsum, s.nv, static_cast<void *>(p->stream)) != 0)
         return fail(HPCGX_ECOMM, "the sum function failed");
@@ -1165,12 +1286,9 @@ Runner group_runner(hpcgx_group *g) {
 // (environment, default 600): on a sharded problem a rank whose peer has
 // failed then returns HPCGX_ETIMEOUT instead of blocking for ever behind an
 // exchange.  The queued work itself is left to finish.
-int bounded_wait(cudaStream_t s) {
-  static const double limit = [] {
-    const char *e = std::getenv("HPCGX_WAIT_TIMEOUT_S");
-    const double v = e ? std::atof(e) : 0.0;
-    return v > 0.0 ? v : 600.0;
-  }();
+int bounded_wait(hpcgx_problem *p) {
+  const double limit = wait_limit_s();
+  cudaStream_t s = p->stream;
   cudaEvent_t ev;
   CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   cudaError_t e = cudaEventRecord(ev, s);
@@ -1184,8 +1302,13 @@ int bounded_wait(cudaStream_t s) {
     if (now_s() - t0 > limit) {
       cudaEventDestroy(ev);
       cudaGetLastError();           // the not-ready status of the last query
+      // an NCCL kernel waiting for a failed peer would never finish: abort the
+      // communicator, which ends its kernels (attach a new one to go on)
+      const bool nccl = p->nccl && !p->nccl->aborted;
+      if (nccl) nccl_abort(p->nccl);
       return fail(HPCGX_ETIMEOUT, "sharded work did not finish within HPCGX_WAIT_TIMEOUT_S = " +
-                                      std::to_string(limit) + " s");
+                                      std::to_string(limit) + " s" +
+                                      (nccl ? "; the NCCL communicator was aborted" : ""));
     }
     if (polls > 2000) std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
@@ -1228,7 +1351,7 @@ int sharded_cg(const std::vector<hpcgx_problem *> &ps, const Runner &run, int ki
   while (true) {
     // wait (bounded) first: a copy to pageable host memory would block
     // without limit until the stream drains
-    TRY(bounded_wait(p0->stream));
+    TRY(bounded_wait(p0));
     CK(cudaMemcpyAsync(&h, p0->st, sizeof(h), cudaMemcpyDeviceToHost, p0->stream));
     CK(cudaStreamSynchronize(p0->stream));   // idle stream: returns at once
     if (h.done) break;
@@ -1237,8 +1360,7 @@ int sharded_cg(const std::vector<hpcgx_problem *> &ps, const Runner &run, int ki
   for (size_t r = 0; r < P; ++r)
     CK(cudaMemcpyAsync(x[r], ps[r]->x, ps[r]->L[0].n * sizeof(double), cudaMemcpyDeviceToDevice,
                        ps[r]->stream));
-  for (hpcgx_problem *p : ps) TRY(bounded_wait(p->stream));
-  for (hpcgx_problem *p : ps) TRY(p->wave_check());
+  for (hpcgx_problem *p : ps) TRY(bounded_wait(p));
   if (niters) *niters = h.niters;
   if (normr) *normr = h.normr;
   if (normr0) *normr0 = h.normr0;
@@ -1252,8 +1374,7 @@ int sharded_op(const std::vector<hpcgx_problem *> &ps, const Runner &run, BUILD 
   std::vector<Plan> plans(ps.size());
   for (size_t r = 0; r < ps.size(); ++r) TRY(build(ps[r], plans[r], (int)r));
   TRY(run(plans));
-  for (hpcgx_problem *p : ps) TRY(bounded_wait(p->stream));
-  for (hpcgx_problem *p : ps) TRY(p->wave_check());
+  for (hpcgx_problem *p : ps) TRY(bounded_wait(p));
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1304,13 +1425,6 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   hpcgx_problem *p = new hpcgx_problem;
   p->device = device;
   p->nlev = levels;
-  // sweep form: the seven class launches, or with HPCGX_GS_WAVE=1 the
-  // one-launch sweep (bit-identical; slower on B200 at 512^3: 3.79 ms per
-  // finest-level sweep against 3.32 ms), whose stage lag (planes) and item
-  // size (rows) can be tuned
-  p->wave = env_int("HPCGX_GS_WAVE", 0) != 0;
-  const int wave_lag = env_int("HPCGX_WAVE_LAG", 6);
-  const int wave_rows = env_int("HPCGX_WAVE_ROWS", 2048);
   p->nranks = nranks;
   p->rank = rank;
   int rc = HPCGX_OK;
@@ -1321,23 +1435,15 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(cuda_fail(e));
   p->stream = p->own_stream;
+  // reduction scratch: up to two values per block of any reducing launch,
+  // plus two per group of 1024 blocks
+  auto red_need = [](int64_t blocks) { return 2 * blocks + 2 * ((blocks + 1023) / 1024); };
   int64_t red_cap = 0;
   for (int l = 0; l < levels; ++l) {
     LevelDev &A = p->L[l];
     plan_level(A, nx >> l, ny >> l, nz >> l);
     A.zlo = rank > 0;
     A.zhi = rank + 1 < nranks;
-    {
-      const std::vector<int2> tab = wave_plan(A, wave_lag, wave_rows);
-      if (!tab.empty()) {
-        const size_t nctr = (size_t)7 * A.wave_nzq + 3;
-        if ((rc = p->alloc((void **)&A.wave_tab, tab.size() * sizeof(int2)))) return bail(rc);
-        if ((rc = p->alloc((void **)&A.wave_ctr, nctr * sizeof(int)))) return bail(rc);
-        e = cudaMemcpy(A.wave_tab, tab.data(), tab.size() * sizeof(int2), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemset(A.wave_ctr, 0, nctr * sizeof(int));
-        if (e != cudaSuccess) return bail(cuda_fail(e));
-      }
-    }
     const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
     if ((rc = p->alloc((void **)&A.vals, slots * sizeof(double)))) return bail(rc);
     if ((rc = p->alloc((void **)&A.cols, slots * sizeof(int32_t)))) return bail(rc);
@@ -1348,10 +1454,12 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
       if ((rc = p->alloc((void **)&A.r32, A.n * sizeof(float)))) return bail(rc);
       if ((rc = p->alloc_halo((void **)&A.x32, A.n, sizeof(float), plane))) return bail(rc);
     }
-    red_cap = std::max<int64_t>(red_cap, A.spmv_blocks);
+    red_cap = std::max<int64_t>(red_cap, red_need(A.spmv_blocks));
+    for (int q = 0; q < 4; ++q)
+      red_cap = std::max<int64_t>(red_cap, red_need(A.blocks[q]));
   }
   const int64_t n = p->L[0].n;
-  red_cap = 2 * std::max<int64_t>(red_cap, vector_blocks(n));
+  red_cap = std::max<int64_t>(red_cap, red_need(vector_blocks(n)));
   const int64_t plane0 = (int64_t)p->L[0].nx * p->L[0].ny;
   for (double **v : {&p->b, &p->x, &p->r, &p->Ap, &p->tmp})
     if ((rc = p->alloc((void **)v, n * sizeof(double)))) return bail(rc);
@@ -1360,6 +1468,7 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   if ((rc = p->alloc_halo((void **)&p->z32, n, sizeof(float), plane0))) return bail(rc);
   if ((rc = p->alloc((void **)&p->gsum, 2 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->result, 4 * sizeof(double)))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->rz_part, 6 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->st, sizeof(CgState)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->red.partials, red_cap * sizeof(double)))) return bail(rc);
   const int64_t ncounters = 1 + (red_cap + 1023) / 1024;   // top counter + one per group
@@ -1370,6 +1479,67 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   if (e != cudaSuccess) return bail(cuda_fail(e));
   *out = p;
   return HPCGX_OK;
+}
+
+int hpcgx_create_general(int device, int levels, hpcgx_problem **out) {
+  NvtxRange range_("hpcgx_create_general");
+  if (!out) return fail(HPCGX_EINVAL, "null output");
+  *out = nullptr;
+  if (levels < 1 || levels > kMaxLevels) return fail(HPCGX_EINVAL, "bad level count");
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e);
+  hpcgx_problem *p = new hpcgx_problem;
+  p->device = device;
+  p->nlev = levels;
+  e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete p;
+    return cuda_fail(e);
+  }
+  p->stream = p->own_stream;
+  p->gen = general_create(levels, p->stream);
+  *out = p;
+  return HPCGX_OK;
+}
+
+int hpcgx_load_level_general(hpcgx_problem *p, int level, int64_t nrows, const char *nnz,
+                             const int32_t *const *cols, const double *const *vals,
+                             const int32_t *f2c, int64_t nc) {
+  NvtxRange range_("hpcgx_load_level_general");
+  HANDLE(p);
+  if (!p->gen) return fail(HPCGX_ESTATE, "not a general-pattern problem (hpcgx_create_general)");
+  TRY(check_level(p, level));
+  if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null row arrays");
+  CK(cudaSetDevice(p->device));
+  const char *why = nullptr;
+  const int rc = general_load_level(p->gen, level, nrows, nnz, cols, vals, f2c, nc, &why);
+  if (rc == HPCGX_ELAYOUT) return fail(rc, why ? why : "matrix rejected");
+  if (rc != HPCGX_OK) return rc;
+  p->L[level].n = nrows;
+  if (level == 0) {
+    // the vectors and reduction scratch of the shared entry points (host
+    // staging, dot, WAXPBY, residual, CG's b and x)
+    for (double **v : {&p->b, &p->x})
+      TRY(p->alloc((void **)v, nrows * sizeof(double)));
+    TRY(p->alloc((void **)&p->result, 4 * sizeof(double)));
+    const int64_t blocks = vector_blocks(nrows);
+    const int64_t cap = 2 * blocks + 2 * ((blocks + 1023) / 1024);
+    TRY(p->alloc((void **)&p->red.partials, cap * sizeof(double)));
+    const int64_t counters = 1 + (cap + 1023) / 1024;
+    TRY(p->alloc((void **)&p->red.counter, counters * sizeof(unsigned int)));
+    p->red.capacity = cap;
+    CK(cudaMemsetAsync(p->red.counter, 0, counters * sizeof(unsigned int), p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+  }
+  p->loaded[level] = true;
+  return HPCGX_OK;
+}
+
+int hpcgx_colours(hpcgx_problem *p, int level) {
+  HANDLE(p);
+  TRY(check_level(p, level));
+  if (!p->gen) return 8;   // the stencil layout's parity colouring
+  return general_colours(p->gen, level);
 }
 
 int hpcgx_destroy(hpcgx_problem *p) {
@@ -1387,6 +1557,7 @@ int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz, const int3
                      const double *vals) {
   NvtxRange range_("hpcgx_load_level");
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_load_level"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "sharded problems are generated on the device");
   if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
   return load_level_impl(
@@ -1401,6 +1572,7 @@ int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz,
                           const int32_t *const *cols, const double *const *vals) {
   NvtxRange range_("hpcgx_load_level_rows");
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_load_level_rows"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "sharded problems are generated on the device");
   if (!nnz || !cols || !vals) return fail(HPCGX_EINVAL, "null host array");
   return load_level_impl(
@@ -1413,6 +1585,7 @@ int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz,
 
 int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c, int64_t nc) {
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_check_f2c"));
   TRY(check_level(p, level));
   if (level + 1 >= p->nlev) return fail(HPCGX_EINVAL, "coarsest level has no injection");
   const LevelDev &F = p->L[level];
@@ -1429,6 +1602,7 @@ int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c, int64_t nc)
 int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma) {
   NvtxRange range_("hpcgx_generate");
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_generate"));
   for (int l = 0; l < p->nlev; ++l) {
     if (kind == HPCGX_GEN_HPCG) {
       p->note(launch_generate_hpcg(p->L[l], p->stream));
@@ -1449,14 +1623,34 @@ int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma) {
 int hpcgx_build_mixed(hpcgx_problem *p) {
   NvtxRange range_("hpcgx_build_mixed");
   HANDLE(p);
+  TRY(stencil_only(p, "the mixed-precision solver"));
   p->mixed_stale = true;
   TRY(p->check_ready(true));
   CK(cudaStreamSynchronize(p->stream));
   return HPCGX_OK;
 }
 
+int hpcgx_set_stencil_columns(hpcgx_problem *p, int on) {
+  HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_set_stencil_columns"));
+  for (int l = 0; l < p->nlev; ++l) p->L[l].stencil_cols = on != 0;
+  // the FP64 iteration graphs hold the other kernels: rebuild them on next use
+  for (int k : {G_FP64_PREC, G_FP64_NOPREC})
+    if (p->graph[k]) {
+      CK(cudaGraphExecDestroy(p->graph[k]));
+      p->graph[k] = nullptr;
+      p->probes[k].clear();
+    }
+  return HPCGX_OK;
+}
+
 int hpcgx_set_diagonal_host(hpcgx_problem *p, int level, const double *diag) {
   HANDLE(p);
+  if (p->gen) {
+    TRY(check_level(p, level));
+    TRY(general_ready_or_fail(p));
+    return general_set_diagonal(p->gen, level, diag);
+  }
   TRY(check_level(p, level));
   const LevelDev &A = p->L[level];
   CK(cudaMemcpyAsync(p->tmp, diag, A.n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
@@ -1468,6 +1662,11 @@ int hpcgx_set_diagonal_host(hpcgx_problem *p, int level, const double *diag) {
 
 int hpcgx_get_diagonal_host(hpcgx_problem *p, int level, double *diag) {
   HANDLE(p);
+  if (p->gen) {
+    TRY(check_level(p, level));
+    TRY(general_ready_or_fail(p));
+    return general_get_diagonal(p->gen, level, diag);
+  }
   TRY(check_level(p, level));
   const LevelDev &A = p->L[level];
   p->note(launch_get_diagonal(A, p->tmp, p->stream));
@@ -1479,6 +1678,7 @@ int hpcgx_get_diagonal_host(hpcgx_problem *p, int level, double *diag) {
 int hpcgx_set_values(hpcgx_problem *p, int level, const double *vals27, int recoarsen) {
   NvtxRange range_("hpcgx_set_values");
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_set_values"));
   TRY(check_level(p, level));
   p->note(launch_set_values(p->L[level], vals27, p->stream));
   p->loaded[level] = true;
@@ -1495,6 +1695,7 @@ int hpcgx_set_values(hpcgx_problem *p, int level, const double *vals27, int reco
 
 int hpcgx_get_values(hpcgx_problem *p, int level, double *vals27, int32_t *cols27) {
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_get_values"));
   TRY(check_level(p, level));
   p->note(launch_get_values(p->L[level], vals27, cols27, p->stream));
   CK(cudaStreamSynchronize(p->stream));
@@ -1503,13 +1704,18 @@ int hpcgx_get_values(hpcgx_problem *p, int level, double *vals27, int32_t *cols2
 
 int hpcgx_memory_bytes(hpcgx_problem *p, double *bytes) {
   if (!p || !bytes) return fail(HPCGX_EINVAL, "null argument");
-  *bytes = (double)p->bytes;
+  *bytes = (double)p->bytes + (p->gen ? general_bytes(p->gen) : 0.0);
   return HPCGX_OK;
 }
 
 int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
   NvtxRange range_("hpcgx_spmv");
   HANDLE(p);
+  if (p->gen) {
+    TRY(check_level(p, level));
+    TRY(general_ready_or_fail(p));
+    return general_spmv(p->gen, level, x, y);
+  }
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
   if (p->sharded()) {
@@ -1527,6 +1733,7 @@ int hpcgx_spmv(hpcgx_problem *p, int level, const double *x, double *y) {
 int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y) {
   NvtxRange range_("hpcgx_spmv_stencil");
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_spmv_stencil"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
@@ -1539,6 +1746,11 @@ int hpcgx_spmv_stencil(hpcgx_problem *p, int level, const double *x, double *y) 
 int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
   NvtxRange range_("hpcgx_symgs");
   HANDLE(p);
+  if (p->gen) {
+    TRY(check_level(p, level));
+    TRY(general_ready_or_fail(p));
+    return general_symgs(p->gen, level, r, x);
+  }
   TRY(check_level(p, level));
   if (!p->loaded[level]) return fail(HPCGX_ESTATE, "level not loaded");
   if (p->sharded()) {
@@ -1549,7 +1761,6 @@ int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
   }
   TRY((p->symgs<double, double>(level, r, x)));
   CK(cudaStreamSynchronize(p->stream));
-  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1557,6 +1768,10 @@ int hpcgx_symgs(hpcgx_problem *p, int level, const double *r, double *x) {
 int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
   NvtxRange range_("hpcgx_mg");
   HANDLE(p);
+  if (p->gen) {
+    TRY(general_ready_or_fail(p));
+    return general_mg(p->gen, r, x);
+  }
   TRY(p->check_ready(false));
   if (p->sharded()) {
     TRY(need_comm(p));
@@ -1566,7 +1781,6 @@ int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
   }
   TRY((p->vcycle<double, double>(r, x, nullptr)));
   CK(cudaStreamSynchronize(p->stream));
-  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1574,6 +1788,7 @@ int hpcgx_mg(hpcgx_problem *p, const double *r, double *x) {
 int hpcgx_spmv_mixed(hpcgx_problem *p, int level, const float *x, float *y) {
   NvtxRange range_("hpcgx_spmv_mixed");
   HANDLE(p);
+  TRY(stencil_only(p, "the mixed-precision solver"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
   TRY(p->check_ready(true));
@@ -1587,6 +1802,7 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
                       float *x) {
   NvtxRange range_("hpcgx_symgs_mixed");
   HANDLE(p);
+  TRY(stencil_only(p, "the mixed-precision solver"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(check_level(p, level));
   TRY(p->check_ready(true));
@@ -1596,7 +1812,6 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
   else
     TRY((p->symgs<float, float>(level, r32, x)));
   CK(cudaStreamSynchronize(p->stream));
-  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1604,11 +1819,11 @@ int hpcgx_symgs_mixed(hpcgx_problem *p, int level, const double *r64, const floa
 int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x) {
   NvtxRange range_("hpcgx_mg_mixed");
   HANDLE(p);
+  TRY(stencil_only(p, "the mixed-precision solver"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   TRY(p->check_ready(true));
   TRY((p->vcycle<float, double>(r, x, nullptr)));
   CK(cudaStreamSynchronize(p->stream));
-  TRY(p->wave_check());
   CK(cudaGetLastError());
   return HPCGX_OK;
 }
@@ -1616,6 +1831,7 @@ int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x) {
 int hpcgx_restriction(hpcgx_problem *p, int level, const double *rf, const double *Axf,
                       double *rc) {
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_restriction"));
   TRY(check_level(p, level));
   if (level + 1 >= p->nlev) return fail(HPCGX_EINVAL, "coarsest level has no restriction");
   p->note(launch_restriction(p->L[level + 1].n, p->L[level], rf, Axf, rc, p->stream));
@@ -1626,6 +1842,7 @@ int hpcgx_restriction(hpcgx_problem *p, int level, const double *rf, const doubl
 
 int hpcgx_prolongation(hpcgx_problem *p, int level, const double *xc, double *xf) {
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_prolongation"));
   TRY(check_level(p, level));
   if (level + 1 >= p->nlev) return fail(HPCGX_EINVAL, "coarsest level has no prolongation");
   p->note(launch_prolongation(p->L[level + 1].n, p->L[level], xc, xf, p->stream));
@@ -1667,6 +1884,10 @@ int hpcgx_cg(hpcgx_problem *p, const double *b, double *x, int max_iter, double 
              int precond, int *niters, double *normr, double *normr0, double *times) {
   NvtxRange range_("hpcgx_cg");
   HANDLE(p);
+  if (p->gen) {
+    TRY(general_ready_or_fail(p));
+    return general_cg(p->gen, b, x, max_iter, tolerance, precond, niters, normr, normr0, times);
+  }
   if (p->sharded()) {
     TRY(need_comm(p));
     return sharded_cg({p}, single_runner(p), precond ? G_FP64_PREC : G_FP64_NOPREC, &b, &x,
@@ -1680,6 +1901,7 @@ int hpcgx_cg_mixed(hpcgx_problem *p, const double *b, double *x, int max_iter, d
                    int *niters, double *normr, double *normr0, double *times) {
   NvtxRange range_("hpcgx_cg_mixed");
   HANDLE(p);
+  TRY(stencil_only(p, "the mixed-precision solver"));
   if (p->sharded()) {
     TRY(need_comm(p));
     return sharded_cg({p}, single_runner(p), G_MIXED, &b, &x, max_iter, tolerance, niters, normr,
@@ -1700,9 +1922,14 @@ int hpcgx_cg_host(hpcgx_problem *p, int mode, const double *b_host, double *x_ho
     case HPCGX_CG_MIXED: kind = G_MIXED; break;
     default: return fail(HPCGX_EINVAL, "unknown CG mode");
   }
+  if (p->gen && kind == G_MIXED) return stencil_only(p, "the mixed-precision solver");
+  if (p->gen) TRY(general_ready_or_fail(p));
   CK(cudaMemcpyAsync(p->b, b_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
   CK(cudaMemcpyAsync(p->x, x_host, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
-  if (p->sharded()) {
+  if (p->gen) {
+    TRY(general_cg(p->gen, p->b, p->x, max_iter, tolerance, kind == G_FP64_PREC, niters, normr,
+                   normr0, times));
+  } else if (p->sharded()) {
     TRY(need_comm(p));
     const double *bd = p->b;
     double *xd = p->x;
@@ -1770,6 +1997,7 @@ int hpcgx_waxpby_host(hpcgx_problem *p, int64_t n, double alpha, const double *x
 int hpcgx_adjoint_grad(hpcgx_problem *p, const double *lambda, const double *x, double *grad) {
   NvtxRange range_("hpcgx_adjoint_grad");
   HANDLE(p);
+  TRY(stencil_only(p, "hpcgx_adjoint_grad"));
   if (p->nranks > 1) return fail(HPCGX_ESTATE, "not available on a sharded problem");
   p->note(launch_adjoint_grad(p->L[0], lambda, x, grad, p->stream));
   CK(cudaStreamSynchronize(p->stream));
@@ -1821,12 +2049,25 @@ int hpcgx_probe_read(hpcgx_problem *p, int kind, double *ms, int64_t *launches, 
   return HPCGX_OK;
 }
 
-int64_t hpcgx_launch_count(hpcgx_problem *p) { return p ? p->launches : -1; }
+int64_t hpcgx_launch_count(hpcgx_problem *p) {
+  return p ? p->launches + (p->gen ? general_launches(p->gen) : 0) : -1;
+}
+
+int hpcgx_iteration_bytes(hpcgx_problem *p, int mode, double *bytes) {
+  HANDLE(p);
+  if (!bytes) return fail(HPCGX_EINVAL, "null output");
+  int kind = 0;
+  TRY(group_kind(mode, &kind));
+  if (!p->graph[kind]) return fail(HPCGX_ESTATE, "no solve of this mode has run on the problem yet");
+  *bytes = p->graph_bytes[kind];
+  return HPCGX_OK;
+}
 
 int hpcgx_set_stream(hpcgx_problem *p, void *stream) {
   HANDLE(p);
   CK(cudaStreamSynchronize(p->stream));
   p->stream = stream ? static_cast<cudaStream_t>(stream) : p->own_stream;
+  if (p->gen) general_set_stream(p->gen, p->stream);
   return HPCGX_OK;
 }
 
@@ -1838,10 +2079,6 @@ int hpcgx_synchronize(hpcgx_problem *p) {
 
 int hpcgx_check_status(void) {
   CK(cudaDeviceSynchronize());
-  unsigned int wf = 0u;
-  const int we = read_wave_fault(&wf);
-  if (we != 0) return cuda_fail((cudaError_t)we);
-  if (wf) return fail(HPCGX_ETIMEOUT, "a one-launch Gauss-Seidel sweep gave up waiting for a stage");
   unsigned long long rec = 0ull;
   const int e = read_check_record(&rec);
   if (e != 0) return cuda_fail((cudaError_t)e);
@@ -1855,36 +2092,14 @@ int hpcgx_check_status(void) {
                                 " index " + std::to_string(index) + " out of range");
 }
 
-int hpcgx_wave_schedule(int nx, int ny, int nz, int lag, int rows_per_item, int cap, int *codes,
-                        int *starts, int *count, int *total, int *lines_per_item,
-                        int *items_per_plane) {
-  if (nx < 1 || ny < 1 || nz < 1 || cap < 0 || !count || !total || !lines_per_item ||
-      !items_per_plane || (cap > 0 && (!codes || !starts)))
-    return fail(HPCGX_EINVAL, "bad arguments");
-  if ((int64_t)nx * ny * (nz + 2) >= (int64_t)1 << 31)
-    return fail(HPCGX_EINVAL, "more than 2^31 rows");
-  LevelDev L;
-  plan_level(L, nx, ny, nz);
-  const std::vector<int2> tab = wave_plan(L, lag, rows_per_item);
-  *count = (int)tab.size();
-  *total = L.wave_total;
-  *lines_per_item = L.wave_lpi;
-  for (int q = 0; q < 4; ++q) items_per_plane[q] = L.wave_ipp[q];
-  if ((int)tab.size() > cap) return fail(HPCGX_EINVAL, "table larger than cap");
-  for (size_t i = 0; i < tab.size(); ++i) {
-    codes[i] = tab[i].x;
-    starts[i] = tab[i].y;
-  }
-  return HPCGX_OK;
-}
-
 // ---- sharding
 int hpcgx_nccl_unique_id(void *id, int bytes) {
   if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");
   NcclApi *api = nccl_api();
   if (!api) return fail(HPCGX_ECOMM, "NCCL (libnccl.so.2) could not be loaded");
   ncclUniqueId u;
-  NCCLCK(api->GetUniqueId(&u));
+  const ncclResult_t r = api->GetUniqueId(&u);
+  if (r != ncclSuccess) return fail(HPCGX_ECOMM, std::string("ncclGetUniqueId: ") + api->GetErrorString(r));
   std::memcpy(id, &u, sizeof(u));
   return HPCGX_OK;
 }
@@ -1892,7 +2107,12 @@ int hpcgx_nccl_unique_id(void *id, int bytes) {
 int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
   NvtxRange range_("hpcgx_attach_nccl");
   HANDLE(p);
+  TRY(stencil_only(p, "sharding"));
   if (!id || bytes < (int)sizeof(ncclUniqueId)) return fail(HPCGX_EINVAL, "id buffer too small");
+  if (p->nccl && p->nccl->aborted) {   // a communicator aborted on a timeout: replace it
+    nccl_release(p->nccl);
+    p->nccl = nullptr;
+  }
   if (p->nccl || p->comm_halo) return fail(HPCGX_ESTATE, "a communicator is attached already");
   NcclApi *api = nccl_api();
   if (!api) return fail(HPCGX_ECOMM, "NCCL (libnccl.so.2) could not be loaded");
@@ -1900,10 +2120,17 @@ int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
   std::memcpy(&u, id, sizeof(u));
   CK(cudaSetDevice(p->device));
   NcclLink *link = new NcclLink;
-  ncclResult_t r = api->CommInitRank(&link->comm, p->nranks, u, p->rank);
-  if (r != ncclSuccess) {
+  ncclConfig_t config = NCCL_CONFIG_INITIALIZER;
+  config.blocking = 0;
+  ncclResult_t r = api->CommInitRankConfig(&link->comm, p->nranks, u, p->rank, &config);
+  if (r != ncclSuccess && r != ncclInProgress) {
     delete link;
-    return fail(HPCGX_ECOMM, std::string("ncclCommInitRank: ") + api->GetErrorString(r));
+    return fail(HPCGX_ECOMM, std::string("ncclCommInitRankConfig: ") + api->GetErrorString(r));
+  }
+  const int rc = nccl_settle(link, r, "ncclCommInitRankConfig");
+  if (rc != HPCGX_OK) {
+    nccl_release(link);
+    return rc;
   }
   p->nccl = link;
   return HPCGX_OK;
@@ -1911,6 +2138,7 @@ int hpcgx_attach_nccl(hpcgx_problem *p, const void *id, int bytes) {
 
 int hpcgx_attach_comm(hpcgx_problem *p, hpcgx_halo_fn halo, hpcgx_sum_fn sum, void *ctx) {
   HANDLE(p);
+  TRY(stencil_only(p, "sharding"));
   if (!halo || !sum) return fail(HPCGX_EINVAL, "both functions are needed");
   if (p->nccl || p->comm_halo) return fail(HPCGX_ESTATE, "a communicator is attached already");
   p->comm_halo = halo;

@@ -1,12 +1,19 @@
 // OptimizeProblem.cpp (drop-in) -- builds the device layout of every level.
 //
 // Replaces src/OptimizeProblem.cpp (interface src/OptimizeProblem.hpp:22,28).
-// Each level's rows (nonzerosInRow / mtxIndL / matrixValues) are uploaded into
-// libhpcgx's colour-sorted sliced-ELL layout; the multicolouring is the
-// 8-colour (ix, iy, iz parity) colouring that the reference's greedy
-// colouring (src/OptimizeProblem.cpp:43-96) produces on this stencil.  The
-// injection operators are checked against the geometric injection the
-// kernels use.  The time spent here is charged by the driver to times[7].
+// Two layouts, chosen per problem by checking the matrix:
+//   * every level is the 27-point stencil matrix of its geometry (entries in
+//     stencil order) and every injection operator is the geometric one: the
+//     rows (nonzerosInRow / mtxIndL / matrixValues) are uploaded into
+//     libhpcgx's colour-sorted stencil layout, whose 8-colour (ix, iy, iz
+//     parity) colouring is what the reference's greedy colouring
+//     (src/OptimizeProblem.cpp:50-79) produces on this matrix;
+//   * anything else -- the reference asks that "any code must work for general
+//     unstructured sparse matrices" (src/GenerateProblem.cpp:47-49) -- goes to a
+//     general-pattern problem (hpcgx_create_general): the greedy colouring
+//     computed from the matrix graph, stored columns, the given f2c.
+// HPCGX_DROPIN_GENERAL=1 takes the general path for every matrix.  The time
+// spent here is charged by the driver to times[7].
 #include "OptimizeProblem.hpp"
 
 #include <cstdlib>
@@ -37,17 +44,43 @@ int OptimizeProblem(SparseMatrix &A, CGData &data, Vector &b, Vector &x, Vector 
   int levels = 1;
   for (const SparseMatrix *m = &A; m->mgData; m = m->Ac) ++levels;
   const char *dev = std::getenv("HPCGX_DEVICE");
+  const int device = dev ? std::atoi(dev) : 0;
+  const char *gen = std::getenv("HPCGX_DROPIN_GENERAL");
   hpcgx_problem *p = nullptr;
-  int rc = hpcgx_create(dev ? std::atoi(dev) : 0, A.geom->nx, A.geom->ny, A.geom->nz, levels, &p);
-  if (rc != HPCGX_OK) return hpcgx_dropin::report(rc, "OptimizeProblem: hpcgx_create");
+  int rc = HPCGX_ELAYOUT;
+  if (!(gen && gen[0] == '1')) {
+    // the stencil layout, if every level and injection is the stencil's
+    rc = hpcgx_create(device, A.geom->nx, A.geom->ny, A.geom->nz, levels, &p);
+    if (rc != HPCGX_OK) return hpcgx_dropin::report(rc, "OptimizeProblem: hpcgx_create");
+    int level = 0;
+    for (SparseMatrix *m = &A; m && rc == HPCGX_OK; m = m->Ac, ++level) {
+      rc = hpcgx_load_level_rows(p, level, m->nonzerosInRow, m->mtxIndL, m->matrixValues);
+      if (rc == HPCGX_OK && m->mgData)
+        rc = hpcgx_check_f2c(p, level, m->mgData->f2cOperator, m->mgData->rc->localLength);
+    }
+    if (rc != HPCGX_OK && rc != HPCGX_ELAYOUT)
+      return hpcgx_dropin::report(rc, "OptimizeProblem: stencil layout");
+    if (rc == HPCGX_ELAYOUT) {
+      HPCG_fout << "OptimizeProblem: not the 27-point stencil layout (" << hpcgx_last_error()
+                << "); using the general-pattern layout" << std::endl;
+      hpcgx_destroy(p);
+      p = nullptr;
+    }
+  }
+  if (!p) {
+    rc = hpcgx_create_general(device, levels, &p);
+    if (rc != HPCGX_OK) return hpcgx_dropin::report(rc, "OptimizeProblem: hpcgx_create_general");
+    int level = 0;
+    for (SparseMatrix *m = &A; m; m = m->Ac, ++level) {
+      const int32_t *f2c = m->mgData ? m->mgData->f2cOperator : nullptr;
+      const int64_t nc = m->mgData ? m->mgData->rc->localLength : 0;
+      rc = hpcgx_load_level_general(p, level, m->localNumberOfRows, m->nonzerosInRow,
+                                    m->mtxIndL, m->matrixValues, f2c, nc);
+      if (rc != HPCGX_OK) return hpcgx_dropin::report(rc, "OptimizeProblem: hpcgx_load_level_general");
+    }
+  }
   int level = 0;
   for (SparseMatrix *m = &A; m; m = m->Ac, ++level) {
-    rc = hpcgx_load_level_rows(p, level, m->nonzerosInRow, m->mtxIndL, m->matrixValues);
-    if (rc != HPCGX_OK) return hpcgx_dropin::report(rc, "OptimizeProblem: hpcgx_load_level_rows");
-    if (m->mgData) {
-      rc = hpcgx_check_f2c(p, level, m->mgData->f2cOperator, m->mgData->rc->localLength);
-      if (rc != HPCGX_OK) return hpcgx_dropin::report(rc, "OptimizeProblem: hpcgx_check_f2c");
-    }
     hpcgx_dropin::LevelState *s = new hpcgx_dropin::LevelState;
     s->problem = p;
     s->level = level;

@@ -2,8 +2,8 @@
 every non-replaceable source file, compiled where they lie) linked with the
 drop-in operator files of this directory and libhpcgx.so.
 
-Needs the reference sources (HPCG_REF_SRC, default /root/reference/src); the
-binary is written to _build/ next to this file and found by tests through
+Needs the reference's src/ directory in the environment variable HPCG_REF_SRC;
+the binary is written to _build/ next to this file and found by tests through
 BINARY.  Without the sources nothing is built.
 """
 from __future__ import annotations
@@ -15,7 +15,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
-REF = os.environ.get("HPCG_REF_SRC", "/root/reference/src")
+REF = os.environ.get("HPCG_REF_SRC", "")
 BINARY = os.path.join(HERE, "_build", "xhpcg_b200")
 # The files HPCG expects an implementation to replace (src/*.cpp forwarding to
 # *_ref); GenerateProblem.cpp is replaced to cut set-up time (same data).
@@ -25,7 +25,7 @@ REPLACED = ["CG.cpp", "ComputeSPMV.cpp", "ComputeSYMGS.cpp", "ComputeMG.cpp",
 
 
 def build(force: bool = False) -> str | None:
-    if not os.path.exists(os.path.join(REF, "main.cpp")):
+    if not REF or not os.path.exists(os.path.join(REF, "main.cpp")):
         return None
     from hpcg_b200 import build as hb
     lib = hb.build()

@@ -56,6 +56,44 @@ class Problem:
         check(lib().hpcgx_set_stream(self.h, C.c_void_p(self.stream.cuda_stream)))
         self.values_version = 0     # bumped whenever matrix values change
 
+    @classmethod
+    def general(cls, levels=4, device=0):
+        """A general-pattern problem (hpcgx_create_general): each level is
+        loaded as given with :meth:`load_level_general` -- any sparsity
+        pattern, the multicolouring computed from the matrix graph."""
+        if not torch.cuda.is_available():
+            raise RuntimeError("hpcg_b200 needs a CUDA device")
+        self = cls.__new__(cls)
+        self.dims = None
+        self.levels = levels
+        self.nranks, self.rank = 1, 0
+        self.device = torch.device("cuda", device)
+        h = C.c_void_p()
+        check(lib().hpcgx_create_general(device, levels, C.byref(h)))
+        self.h = h
+        self.stream = torch.cuda.Stream(device=self.device)
+        check(lib().hpcgx_set_stream(self.h, C.c_void_p(self.stream.cuda_stream)))
+        self.values_version = 0
+        return self
+
+    def load_level_general(self, level, nnz, cols, vals, f2c=None):
+        """Rows of any pattern: row i holds nnz[i] entries in cols[i, :nnz[i]] /
+        vals[i, :nnz[i]] (2-D arrays, one row per matrix row, entries in the
+        order the row sums them); f2c: the injection to the next level."""
+        nnz = np.ascontiguousarray(nnz, np.uint8)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        n, w = cols.shape
+        cptr = (C.c_void_p * n)(*(cols.ctypes.data + 4 * w * np.arange(n)).tolist())
+        vptr = (C.c_void_p * n)(*(vals.ctypes.data + 8 * w * np.arange(n)).tolist())
+        fc = None if f2c is None else np.ascontiguousarray(f2c, np.int32)
+        check(lib().hpcgx_load_level_general(self.h, level, n, _ptr(nnz), cptr, vptr, _ptr(fc),
+                                             0 if fc is None else fc.size))
+        self.values_version += 1
+
+    def colours(self, level=0):
+        return int(lib().hpcgx_colours(self.h, level))
+
     # ----------------------------------------------------------- lifetime
     def close(self):
         if getattr(self, "h", None):
@@ -151,6 +189,8 @@ class Problem:
         self.attach_comm(halo, sum_)
 
     def level_dims(self, level=0):
+        if self.dims is None:
+            raise ValueError("a general-pattern problem has no grid")
         nx, ny, nz = self.dims
         return nx >> level, ny >> level, nz >> level
 
@@ -181,6 +221,11 @@ class Problem:
 
     def build_mixed(self):
         check(lib().hpcgx_build_mixed(self.h))
+
+    def set_stencil_columns(self, on=True):
+        """FP64 operators derive their columns from the stencil offsets (the
+        mixed solver always does); same results, no int32 column reads."""
+        check(lib().hpcgx_set_stencil_columns(self.h, int(bool(on))))
 
     def set_diagonal(self, level, diag):
         d = np.ascontiguousarray(diag, np.float64)
@@ -343,6 +388,14 @@ class Problem:
         check(lib().hpcgx_probe_read(self.h, int(kind), C.byref(ms), C.byref(n), C.byref(b),
                                      int(reset)))
         return ms.value, n.value, b.value
+
+    def iteration_bytes(self, mode=_lib.CG_MIXED):
+        """Algorithmic bytes of one CG iteration of ``mode`` (this
+        implementation's byte model, summed over the iteration's launches);
+        available after a solve of that mode."""
+        out = C.c_double()
+        check(lib().hpcgx_iteration_bytes(self.h, int(mode), C.byref(out)))
+        return out.value
 
     def launch_count(self):
         return int(lib().hpcgx_launch_count(self.h))

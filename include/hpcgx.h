@@ -66,6 +66,26 @@ int hpcgx_load_level(hpcgx_problem *p, int level, const uint8_t *nnz_host,
  * (nonzerosInRow, mtxIndL, matrixValues; src/SparseMatrix.hpp:47-50). */
 int hpcgx_load_level_rows(hpcgx_problem *p, int level, const char *nnz_host,
                           const int32_t *const *cols_host, const double *const *vals_host);
+/* General-pattern problems.  The reference requires that an implementation
+ * work for general unstructured sparse matrices (src/GenerateProblem.cpp:47-49,
+ * src/SetupHalo.cpp:45); the loaders above accept only the 27-point stencil
+ * matrix whose structure the fast layout uses.  hpcgx_create_general makes a
+ * problem that takes each level as given: rows of any pattern (each with a
+ * diagonal entry), the injection f2c to the next level (f2c[i] = fine row of
+ * coarse row i, nc coarse rows; NULL on the last level), the multicolouring
+ * computed from the matrix graph by OptimizeProblem's greedy rule
+ * (src/OptimizeProblem.cpp:50-79).  hpcgx_spmv, hpcgx_symgs (colour order),
+ * hpcgx_mg, hpcgx_cg (plain and MG), their *_host forms, the diagonal
+ * accessors and the vector operators work on it; the mixed solver, the
+ * generators, stencil-only operators and sharding return HPCGX_ESTATE.
+ * Rows are the SparseMatrix arrays (nonzerosInRow, mtxIndL, matrixValues;
+ * src/SparseMatrix.hpp:47-50); a malformed row returns HPCGX_ELAYOUT. */
+int hpcgx_create_general(int device, int levels, hpcgx_problem **out);
+int hpcgx_load_level_general(hpcgx_problem *p, int level, int64_t nrows, const char *nnz_host,
+                             const int32_t *const *cols_host, const double *const *vals_host,
+                             const int32_t *f2c_host, int64_t nc);
+/* Colours of a level's multicolouring (8 for the stencil layout). */
+int hpcgx_colours(hpcgx_problem *p, int level);
 /* Checks that a level's injection operator (MGData::f2cOperator,
  * src/MGData.hpp:31) is the geometric injection the kernels use. */
 int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c_host, int64_t nc);
@@ -77,6 +97,13 @@ int hpcgx_check_f2c(hpcgx_problem *p, int level, const int32_t *f2c_host, int64_
 int hpcgx_generate(hpcgx_problem *p, int kind, uint64_t seed, double sigma);
 /* Builds (or refreshes) the BF16 value copies used by the mixed solver. */
 int hpcgx_build_mixed(hpcgx_problem *p);
+/* on != 0: the FP64 operators (SpMV, SYMGS, MG, CG) derive every column from
+ * the level's stencil offsets instead of reading the int32 column arrays, as
+ * the mixed solver always does (no reference counterpart; loaded levels are
+ * 27-point stencil matrices, so the results are the same bits).  This is the
+ * FP64 solve to compare the mixed one with when only the precision differs.
+ * Default off. */
+int hpcgx_set_stencil_columns(hpcgx_problem *p, int on);
 /* Coherence with ReplaceMatrixDiagonal (src/SparseMatrix.hpp:139-145):
  * writes level `level`'s diagonal from host memory. */
 int hpcgx_set_diagonal_host(hpcgx_problem *p, int level, const double *diag_host);
@@ -153,8 +180,10 @@ int hpcgx_mg_mixed(hpcgx_problem *p, const double *r, float *x);
  *     larger n returns HPCGX_EINVAL (use hpcgx_dot);
  *   - x, y: device vectors of the current device; result: one device double;
  *   - runs asynchronously on `stream` (NULL: the legacy default stream);
- *   - the first call on a device looks up the array's device address; make
- *     that first call before any stream capture on that device;
+ *   - the first call on a device (and the first after the device's context
+ *     was torn down and created again, e.g. by cudaDeviceReset) looks up the
+ *     array's device address; make that call before any stream capture on
+ *     that device;
  *   - every call shares the one array, so calls that overlap on the GPU (on
  *     different streams, or from several host threads) race and must not be
  *     issued concurrently. */
@@ -219,6 +248,12 @@ int hpcgx_probe_read(hpcgx_problem *p, int kind, double *ms, int64_t *launches, 
                      int reset);
 /* Kernel launches issued by the library on this problem since creation. */
 int64_t hpcgx_launch_count(hpcgx_problem *p);
+/* Algorithmic bytes of one CG iteration of `mode` (HPCGX_CG_PLAIN / _MG /
+ * _MIXED) as this implementation moves them: every launch of the iteration's
+ * CUDA graph with the probes' byte model (real nonzeros, each vector element
+ * once per launch that reads or writes it).  Available after a solve of that
+ * mode on the one-GPU solver; HPCGX_ESTATE before. */
+int hpcgx_iteration_bytes(hpcgx_problem *p, int mode, double *bytes);
 /* Waits for all work of the problem's stream. */
 int hpcgx_synchronize(hpcgx_problem *p);
 /* Index-checked build (libhpcgx_checked.so, compiled with -DHPCGX_CHECKED):
@@ -227,17 +262,6 @@ int hpcgx_synchronize(hpcgx_problem *p);
  * access itself was redirected into the buffers), else HPCGX_OK.  Synchronises
  * the device.  Always HPCGX_OK in the regular build, which has no checks. */
 int hpcgx_check_status(void);
-/* Diagnostics, host only (no device needed): the ticket table of the
- * one-launch symmetric sweep (k_gs_wave, HPCGX_GS_WAVE=1) of an nx x ny x nz
- * level with the given stage lag (planes) and item size (rows).  Entry i is
- * stage codes[i] >> 16 (0..6: forward classes 0-2, class 3 both ways,
- * backward classes 2-0) on class plane codes[i] & 0xffff, with tickets
- * starts[i] .. starts[i] + items_per_plane[class] - 1.  *count = 0 where the
- * sweep is not available (ny or nz below 2, lag below 2); HPCGX_EINVAL if
- * more than cap entries would be written (*count holds the number needed). */
-int hpcgx_wave_schedule(int nx, int ny, int nz, int lag, int rows_per_item, int cap, int *codes,
-                        int *starts, int *count, int *total, int *lines_per_item,
-                        int *items_per_plane);
 
 /* ---- sharding over ranks (z-slabs) --------------------------------------
  * The reference's MPI decomposition with a process grid of 1 x 1 x nranks

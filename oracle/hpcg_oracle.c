@@ -610,3 +610,107 @@ void or_adjoint_grad(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
       grad[i * OR_STENCIL + j] = j < nnz[i] ? -(lambda[i] * x[cols[i * OR_STENCIL + j]]) : 0.0;
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Matrix-free restatements for benchmark-size grids                         */
+/* ------------------------------------------------------------------------ */
+/* At 256^3 and 512^3 the stored-matrix restatements above need 6 to 50 GB of
+ * host memory.  These functions apply the same reference operators to the
+ * reference problem of src/GenerateProblem_ref.cpp:152-172 with every row
+ * generated where it is used: present neighbours in (sz, sy, sx) order, 26 on
+ * the diagonal and -1 elsewhere.  The arithmetic per row is exactly that of
+ * or_spmv / gs_row / gs_row32 (same terms, same order), so the results are
+ * bit-identical to the stored-matrix functions (checked on small grids by
+ * tests/test_oracle_pin.py).  Rows of one colour are independent (no two are
+ * neighbours), so the loops over a colour's rows run in parallel (OpenMP)
+ * without changing a bit. */
+
+/* Neighbour columns of row (ix, iy, iz) in entry order; returns the count and
+ * the entry index of the diagonal in *diag. */
+static inline int stencil_row(int nx, int ny, int nz, int64_t ix, int64_t iy, int64_t iz,
+                              int64_t *col, int *diag) {
+  const int64_t row = (iz * ny + iy) * nx + ix;
+  int k = 0;
+  for (int sz = -1; sz <= 1; sz++) {
+    if (iz + sz < 0 || iz + sz >= nz) continue;
+    for (int sy = -1; sy <= 1; sy++) {
+      if (iy + sy < 0 || iy + sy >= ny) continue;
+      for (int sx = -1; sx <= 1; sx++) {
+        if (ix + sx < 0 || ix + sx >= nx) continue;
+        const int64_t c = row + sz * (int64_t)nx * ny + sy * (int64_t)nx + sx;
+        if (c == row) *diag = k;
+        col[k++] = c;
+      }
+    }
+  }
+  return k;
+}
+
+/* ComputeSPMV_ref (src/ComputeSPMV_ref.cpp:58-71) on the reference problem. */
+void or_stencil_spmv(int nx, int ny, int nz, const double *x, double *y) {
+  const int64_t n = (int64_t)nx * ny * nz;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++) {
+    const int64_t ix = i % nx, iy = (i / nx) % ny, iz = i / ((int64_t)nx * ny);
+    int64_t col[OR_STENCIL];
+    int dg = 0;
+    const int k = stencil_row(nx, ny, nz, ix, iy, iz, col, &dg);
+    double sum = 0.0;
+    for (int j = 0; j < k; j++) sum += (j == dg ? 26.0 : -1.0) * x[col[j]];
+    y[i] = sum;
+  }
+}
+
+/* One colour's rows, natural order: colour (ix&1) + 2(iy&1) + 4(iz&1). */
+#define OR_FOR_COLOUR(c, body)                                                       \
+  do {                                                                               \
+    const int px_ = (c) & 1, py_ = ((c) >> 1) & 1, pz_ = ((c) >> 2) & 1;             \
+    const int64_t cz_ = (nz - pz_ + 1) / 2, cy_ = (ny - py_ + 1) / 2,                \
+                  cx_ = (nx - px_ + 1) / 2;                                          \
+    _Pragma("omp parallel for schedule(static)")                                     \
+    for (int64_t t_ = 0; t_ < cz_ * cy_ * cx_; t_++) {                               \
+      const int64_t ix = px_ + 2 * (t_ % cx_), iy = py_ + 2 * ((t_ / cx_) % cy_),    \
+                    iz = pz_ + 2 * (t_ / (cx_ * cy_));                               \
+      body                                                                           \
+    }                                                                                \
+  } while (0)
+
+/* ComputeSYMGS_ref (src/ComputeSYMGS_ref.cpp:54-103) on the reference problem
+ * in colour order (forward colours 0..7, backward 7..0): or_symgs with the
+ * order of Oracle.colour_order. */
+void or_stencil_symgs(int nx, int ny, int nz, const double *r, double *x) {
+  for (int pass = 0; pass < 2; pass++)
+    for (int cc = 0; cc < 8; cc++) {
+      const int c = pass == 0 ? cc : 7 - cc;
+      OR_FOR_COLOUR(c, {
+        const int64_t i = (iz * ny + iy) * nx + ix;
+        int64_t col[OR_STENCIL];
+        int dg = 0;
+        const int k = stencil_row(nx, ny, nz, ix, iy, iz, col, &dg);
+        double sum = r[i];
+        for (int j = 0; j < k; j++) sum -= (j == dg ? 26.0 : -1.0) * x[col[j]];
+        sum += x[i] * 26.0;
+        x[i] = sum / 26.0;
+      });
+    }
+}
+
+/* or_symgs32 (BF16 values -- 26 and -1 are exact -- FP32 vectors, fused
+ * multiply-adds) on the reference problem in colour order; r64 is the FP64
+ * right-hand side of the finest level, rounded to FP32 where it is read. */
+void or_stencil_symgs32(int nx, int ny, int nz, const double *r64, float *x) {
+  for (int pass = 0; pass < 2; pass++)
+    for (int cc = 0; cc < 8; cc++) {
+      const int c = pass == 0 ? cc : 7 - cc;
+      OR_FOR_COLOUR(c, {
+        const int64_t i = (iz * ny + iy) * nx + ix;
+        int64_t col[OR_STENCIL];
+        int dg = 0;
+        const int k = stencil_row(nx, ny, nz, ix, iy, iz, col, &dg);
+        float sum = (float)r64[i];
+        for (int j = 0; j < k; j++) sum = fmaf(-(j == dg ? 26.0f : -1.0f), x[col[j]], sum);
+        sum = fmaf(x[i], 26.0f, sum);
+        x[i] = sum / 26.0f;
+      });
+    }
+}

@@ -121,6 +121,11 @@ int64_t or_generate_varcoef(int nx, int ny, int nz, int level, uint64_t seed, do
 void or_adjoint_grad(int64_t nrow, const uint8_t *nnz, const int32_t *cols,
                      const double *lambda, const double *x, double *grad);
 
+/* matrix-free restatements on the reference problem (benchmark-size grids) */
+void or_stencil_spmv(int nx, int ny, int nz, const double *x, double *y);
+void or_stencil_symgs(int nx, int ny, int nz, const double *r, double *x);
+void or_stencil_symgs32(int nx, int ny, int nz, const double *r64, float *x);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,8 @@ class Oracle:
             lib.or_mg.argtypes = [_P, C.c_int, _P, _P]
             lib.or_mg32.argtypes = [_P, C.c_int, _P, _P, _P]
             lib.or_greedy_colour.argtypes = [_I64, _P, _P, _P, _P]
+            for f in ("or_stencil_spmv", "or_stencil_symgs", "or_stencil_symgs32"):
+                getattr(lib, f).argtypes = [C.c_int, C.c_int, C.c_int, _P, _P]
             cls._lib = lib
         return cls._lib
 
@@ -321,6 +323,33 @@ class Oracle:
                                C.byref(nr), C.byref(nr0), _ptr(work), _ptr(z32))
         assert err == 0
         return x, it.value, nr.value, nr0.value
+
+    # ------------------------------------------------- matrix-free (large grids)
+    @classmethod
+    def stencil_spmv(cls, dims, x):
+        """ComputeSPMV_ref on the reference problem of an nx x ny x nz grid,
+        rows generated on the fly (bit-identical to ``spmv``)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        cls.lib().or_stencil_spmv(*dims, _ptr(x), _ptr(y))
+        return y
+
+    @classmethod
+    def stencil_symgs(cls, dims, r, x):
+        """ComputeSYMGS_ref in colour order on the reference problem
+        (bit-identical to ``symgs(..., coloured=True)``)."""
+        x = np.array(x, dtype=np.float64)
+        cls.lib().or_stencil_symgs(*dims, _ptr(np.ascontiguousarray(r, dtype=np.float64)), _ptr(x))
+        return x
+
+    @classmethod
+    def stencil_symgs32(cls, dims, r64, x32):
+        """The mixed FP32/BF16 sweep in colour order on the reference problem
+        (bit-identical to ``symgs32`` with an FP64 right-hand side)."""
+        x = np.array(x32, dtype=np.float32)
+        cls.lib().or_stencil_symgs32(*dims, _ptr(np.ascontiguousarray(r64, dtype=np.float64)),
+                                     _ptr(x))
+        return x
 
     @classmethod
     def adjoint_grad(cls, lev, lam, x):

@@ -142,6 +142,40 @@ def test_against_reference_golden(oracle):
         assert k == g["cgtol_perm_stats"][0] and nr / nr0 <= 1e-10
 
 
+def test_fp64_stencil_columns(grid, oracle):
+    """hpcgx_set_stencil_columns: the FP64 operators with every column derived
+    from the stencil offsets give the same bits as with the stored columns
+    (SpMV, SYMGS on every level, the V-cycle) and CG_ref's iteration count."""
+    from hpcg_b200 import Problem
+    L, b, xe, _ = setup(grid, oracle)
+    P = Problem(*grid)
+    try:
+        P.generate("hpcg")
+        P.set_stencil_columns(True)
+        u, r, x0 = seeded(oracle, L[0].nrow)
+        for l, lev in enumerate(L):
+            n = lev.nrow
+            assert (host(P.spmv(cuda(u[:n]), level=l)) == oracle.spmv(lev, u[:n])).all()
+            x = cuda(x0[:n])
+            P.symgs(cuda(r[:n]), x, level=l)
+            assert (host(x) == oracle.symgs(lev, r[:n], x0[:n], coloured=True)).all()
+        assert (host(P.mg(cuda(r))) == oracle.mg(L, r, coloured=True)).all()
+        n = L[0].nrow
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        k, nr, nr0 = P.cg(cuda(b), x, 500, 1e-10)
+        _, ok, _, _ = oracle.cg(L, b, np.zeros(n), 500, 1e-10, coloured=True)
+        assert k == ok and nr / nr0 <= 1e-10
+        # and back to the stored columns: the rebuilt iteration graph agrees (the
+        # stencil-column SpMV takes two line groups per block, so its fused p.Ap
+        # sums its partials in another order: norms agree to 1e-6, not bitwise)
+        P.set_stencil_columns(False)
+        x.zero_()
+        k2, nr2, _ = P.cg(cuda(b), x, 500, 1e-10)
+        assert k2 == k and abs(nr2 / nr - 1) < 1e-6
+    finally:
+        P.close()
+
+
 def test_restriction_prolongation_bitexact(grid, oracle):
     L, b, xe, P = setup(grid, oracle)
     u, r, x0 = seeded(oracle, L[0].nrow)
@@ -178,6 +212,12 @@ def test_cg_matches_oracle(grid, oracle):
     ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 10, 0.0, coloured=True)
     assert k == ok == 10
     assert abs(nr0 / onr0 - 1) < 1e-14 and abs(nr / onr - 1) < 1e-8
+    # max_iter = 0: no iteration, both norms are the initial residual norm
+    # (src/CG.cpp:89-96 sets them before the loop)
+    x.zero_()
+    k, nr, nr0 = P.cg(cuda(b), x, 0, 1e-10)
+    assert k == 0 and nr == nr0 and abs(nr0 / onr0 - 1) < 1e-14
+    assert not host(x).any()
     x.zero_()
     k, nr, nr0 = P.cg(cuda(b), x, 500, 1e-10)
     ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 500, 1e-10, coloured=True)
@@ -256,6 +296,17 @@ def test_mixed_cg(grid, oracle):
     rt = np.linalg.norm(host(cuda(b) - P.spmv(x))) / np.linalg.norm(b)
     assert rt < 1e-9
     assert np.abs(host(x) - 1.0).max() < 1e-6
+    # the trajectory, not only the end point.  r.z and z.Ap are reduced inside
+    # the V-cycle's last four launches (in a fixed order of their own), the
+    # oracle sums sequentially: after 1 and 2 iterations (the second is the
+    # first to use z.Ap and beta) the norms agree to 1e-12; after 10, where the
+    # flexible solver has amplified the rounding differences, to 1e-6.
+    for its, tol in ((1, 1e-12), (2, 1e-12), (10, 1e-6)):
+        x.zero_()
+        k, nr, nr0 = P.cg_mixed(cuda(b), x, its, 0.0)
+        ox, ok, onr, onr0 = oracle.fcg(L, b, np.zeros(n), its, 0.0)
+        assert k == ok == its
+        assert abs(nr0 / onr0 - 1) < 1e-14 and abs(nr / onr - 1) < tol, (its, nr, onr)
 
 
 def test_cg_host_buffers(oracle):

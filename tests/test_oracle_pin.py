@@ -200,3 +200,27 @@ def test_varcoef_cg_against_reference(oracle):
     x2, k2, nr2, nr02, _ = ref.cg(b, np.zeros(n), 500, 1e-12)
     assert k1 == k2 and np.abs(x1 - x2).max() < 1e-12
     ref.close()
+
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (16, 24, 32), (24, 24, 24), (10, 6, 14)],
+                         ids=lambda d: "x".join(map(str, d)))
+def test_matrix_free_restatements_match_stored(dims, oracle):
+    """The matrix-free SpMV / colour-ordered SYMGS (FP64 and the mixed FP32/BF16
+    sweep) that check benchmark-size grids are bit-identical to the stored-matrix
+    restatements pinned above, on even, odd and non-cubic grids."""
+    L, b, x, xe = oracle.hierarchy(*dims, levels=1)
+    oracle.colour_order(L)
+    lev = L[0]
+    u, r, x0 = inputs(oracle, lev.nrow)
+    assert (oracle.stencil_spmv(dims, u) == oracle.spmv(lev, u)).all()
+    assert (oracle.stencil_symgs(dims, r, x0) == oracle.symgs(lev, r, x0, coloured=True)).all()
+    x32 = x0.astype(np.float32)
+    assert (oracle.stencil_symgs32(dims, r, x32) == oracle.symgs32(lev, r, x32)).all()
+    # and against the reference's own ComputeSPMV_ref on the same grid
+    from oracle.oracle import RefProblem
+    if RefProblem.available() and all(d % 8 == 0 for d in dims):   # its 4-level hierarchy
+        R = RefProblem(*dims)
+        try:
+            assert (oracle.stencil_spmv(dims, u) == R.spmv(0, u)).all()
+        finally:
+            R.close()

@@ -185,3 +185,53 @@ def test_sharded_problem_needs_a_backend(oracle):
     with pytest.raises(HPCGXError):
         p.generate("varcoef", seed=2, sigma=1.0)
     p.close()
+
+
+_STALL_SCRIPT = r"""
+import os, sys, torch
+sys.path.insert(0, os.environ["HPCGX_ROOT"])
+from hpcg_b200 import HPCGXError, Problem, nccl_unique_id
+dims = (16, 16, 16)
+ref = Problem(*dims)
+ref.generate("hpcg")
+u = ref.fill_uniform(1, -1.0, 1.0)
+b = ref.spmv(u)
+x = torch.zeros_like(b)
+want = ref.cg(b, x, 500, 1e-10)
+one = Problem(*dims, nranks=1, rank=0)
+one.generate("hpcg")
+try:
+    one.attach_nccl(nccl_unique_id())
+    raise SystemExit("the stalled communicator was not reported")
+except HPCGXError as e:
+    assert e.code == 8, e                      # HPCGX_ETIMEOUT
+    assert "aborted" in str(e), e
+# the problem stays usable; a new communicator replaces the aborted one
+one.attach_nccl(nccl_unique_id())
+x.zero_()
+got = one.cg(b, x, 500, 1e-10)
+assert got == want, (got, want)
+one.close()
+ref.close()
+print("stall-ok")
+"""
+
+
+def test_nccl_stall_times_out_and_aborts(tmp_path):
+    """A communicator that never settles (a peer that has died, faked on the
+    host with HPCGX_FAULT_NCCL_STALL: the first settle of the process sees
+    ncclInProgress for ever) is aborted after HPCGX_WAIT_TIMEOUT_S and the call
+    returns HPCGX_ETIMEOUT; the problem stays usable and a new communicator
+    solves as before.  One rank, so no kernel ever waits for another."""
+    import subprocess
+    import sys
+    from conftest import ROOT
+    # the limit must leave a real communicator time to initialise (about a
+    # second); the faked stall then waits it out once
+    env = dict(os.environ, HPCGX_ROOT=ROOT, HPCGX_WAIT_TIMEOUT_S="10",
+               HPCGX_FAULT_NCCL_STALL="1", NCCL_SOCKET_IFNAME="lo", NCCL_NVLS_ENABLE="0")
+    script = tmp_path / "stall.py"
+    script.write_text(_STALL_SCRIPT)
+    out = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0 and "stall-ok" in out.stdout, out.stdout + out.stderr[-3000:]
