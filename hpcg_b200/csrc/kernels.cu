@@ -537,30 +537,6 @@ k_spmv(LevelMat<VT> A, ClassSet cs, const T *__restrict__ x, T *__restrict__ y, 
 
 // ---------------------------------------------------------------- Gauss-Seidel
 
-// Per-thread sums of a GS_DOT launch: r.z and z.Ap over the rows it finalises.
-struct RzAcc {
-  double rz = 0.0, zap = 0.0;
-};
-
-// End of a GS_DOT launch: the block's sums join the grid reduction; launch
-// slot 3's last block adds the four launches' totals in slot order and runs
-// CG's beta step.
-__device__ __forceinline__ void rz_finish(const RzFuse &f, const RzAcc &acc) {
-  double v[2] = {acc.rz, acc.zap}, tot[2];
-  if (grid_reduce<2>(v, f.red, tot) && threadIdx.x == 0) {
-    if (f.slot < 3) {
-      f.part[2 * f.slot] = tot[0];
-      f.part[2 * f.slot + 1] = tot[1];
-    } else {
-      double t[2];
-      t[0] = ((__ldcg(f.part) + __ldcg(f.part + 2)) + __ldcg(f.part + 4)) + tot[0];
-      t[1] = ((__ldcg(f.part + 1) + __ldcg(f.part + 3)) + __ldcg(f.part + 5)) + tot[1];
-      finish_or_defer<2>(f.red, FIN_CG_RZ, f.st, t);
-    }
-  }
-}
-
-
 // One Gauss-Seidel row update, src/ComputeSYMGS_ref.cpp:72-80:
 //   sum = r_i - sum_j a_ij x_j (diagonal included, slot order); sum += x_i a_ii;
 //   x_i = sum / a_ii.
@@ -583,17 +559,11 @@ __device__ __forceinline__ void rz_finish(const RzFuse &f, const RzAcc &acc) {
 //       its backward update (the first step of the backward sweep): between
 //       the two only x_i changes, so the backward value is recomputed from the
 //       same registers and only that value is stored.
-// VEC (FP32 x, even nx, 8-byte aligned x): an interior row reads the three x
-//       neighbours on each of its 9 neighbouring x-lines with one 8-byte load
-//       of the aligned pair among them and one 4-byte load of the third.
-// DOT:  the new x_i is final (a GS_DOT launch): r_i x_i and, with ap, x_i ap_i
-//       are added to acc.
-template <bool ZERO, bool PRO, bool RES, bool SYM = false, bool STN = false, bool DOT = false,
-          bool VEC = false, class VT, class T, class RT>
+template <bool ZERO, bool PRO, bool RES, bool SYM = false, bool STN = false, class VT, class T,
+          class RT>
 __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, int c,
                                        const RT *__restrict__ r, T *x, const T *__restrict__ xc,
-                                       T *__restrict__ rc, RzAcc *acc = nullptr,
-                                       const double *__restrict__ ap = nullptr) {
+                                       T *__restrict__ rc) {
   RowId id = id0;
   check_row(A, id, 3);
   int32_t col[HPCGX_STENCIL];
@@ -611,8 +581,7 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
   }
   if (IMPLICIT) stencil_cols<true>(A, id, need, col);
   check_cols(A, col, need, 4);
-  const RT rraw = __ldg(r + id.row);
-  const T rhs = vec_to(rraw, T());
+  const T rhs = vec_to(__ldg(r + id.row), T());
   int64_t crow = 0;
   if (PRO || RES) {
     const int nxc = A.nx >> 1, nyc = A.ny >> 1;
@@ -626,41 +595,11 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
   // is skipped below.  The gather itself does not wait for the value: every
   // column is in range.
   T xv[HPCGX_STENCIL];
-  bool gathered = false;
-  if constexpr (VEC && std::is_same<T, float>::value) {
-    const bool interior = id.ix > 0 && id.ix + 1 < A.nx && id.iy > 0 && id.iy + 1 < A.ny &&
-                          (id.iz > 0 || A.zlo) && (id.iz + 1 < A.nz || A.zhi);
-    if (interior) {
-      const int px = c & 1, r32 = (int)id.row;
 #pragma unroll
-      for (int ln = 0; ln < 9; ++ln) {
-        // zero guess: a line other than the row's own is read if its colours
-        // are lower; on the own line the x-neighbours are of colour c ^ 1
-        const bool used = ln == 4 ? (!ZERO || (c & 1)) : need(3 * ln);
-        if (!used) continue;
-        const int b = r32 + A.off[3 * ln + 1];   // the neighbour with dx = 0
-        if (px == 0) {
-          const float2 v = *reinterpret_cast<const float2 *>(x + b);
-          xv[3 * ln] = x[b - 1];
-          xv[3 * ln + 1] = v.x;
-          xv[3 * ln + 2] = v.y;
-        } else {
-          const float2 v = *reinterpret_cast<const float2 *>(x + b - 1);
-          xv[3 * ln] = v.x;
-          xv[3 * ln + 1] = v.y;
-          xv[3 * ln + 2] = x[b + 1];
-        }
-      }
-      gathered = true;
-    }
-  }
-  if (!gathered) {
-#pragma unroll
-    for (int s = 0; s < HPCGX_STENCIL; ++s) {
-      if (s == HPCGX_DIAG_SLOT) continue;
-      if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
-      xv[s] = x[col[s]];
-    }
+  for (int s = 0; s < HPCGX_STENCIL; ++s) {
+    if (s == HPCGX_DIAG_SLOT) continue;
+    if (ZERO && ((c ^ slot_mask(s)) > c)) continue;
+    xv[s] = x[col[s]];
   }
   T sum = rhs;
   const T d = val[HPCGX_DIAG_SLOT];
@@ -687,19 +626,10 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
       sum2 = mac_sub(sum2, val[s], xv[s]);
     }
     sum2 = mac_add(sum2, xn, d);
-    const T xb = rn_div(sum2, d);
-    x[id.row] = xb;
-    if (DOT) {
-      acc->rz += (double)rraw * (double)xb;
-      if (ap) acc->zap += (double)xb * __ldg(ap + id.row);
-    }
+    x[id.row] = rn_div(sum2, d);
     return;
   }
   x[id.row] = xn;
-  if (DOT) {
-    acc->rz += (double)rraw * (double)xn;
-    if (ap) acc->zap += (double)xn * __ldg(ap + id.row);
-  }
   if (RES) {
     T ax = T(0);
 #pragma unroll
@@ -716,13 +646,9 @@ __device__ __forceinline__ void gs_row(const LevelMat<VT> &A, const RowId &id0, 
 template <int MODE, int Q, int DIR, class VT, class T, class RT>
 __device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo &C, int j0, int j1,
                                          const RT *__restrict__ r, T *x,
-                                         const T *__restrict__ xc, T *__restrict__ rc,
-                                         const RzFuse &rz) {
+                                         const T *__restrict__ xc, T *__restrict__ rc) {
   constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0, PRO = (MODE & GS_PROLONG) != 0,
-                 RES = (MODE & GS_RESTRICT) != 0, STN = (MODE & GS_STENCIL) != 0,
-                 DOT = (MODE & GS_DOT) != 0, VEC = (MODE & GS_VEC) != 0;
-  RzAcc acc;
-  const double *ap = (DOT && rz.flex && rz.st->k > 1) ? rz.Ap : nullptr;
+                 RES = (MODE & GS_RESTRICT) != 0, STN = (MODE & GS_STENCIL) != 0;
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
     const int px = DIR ? 1 - half : half;
@@ -731,13 +657,12 @@ __device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo 
     for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
       const RowId id = row_of(C, A.nx, A.ny, px, j0, t);
       if ((PRO || RES) && c == 0)
-        gs_row<ZERO, PRO, RES, false, STN, false, VEC>(A, id, c, r, x, xc, rc);
+        gs_row<ZERO, PRO, RES, false, STN>(A, id, c, r, x, xc, rc);
       else
-        gs_row<ZERO, false, false, false, STN, DOT, VEC>(A, id, c, r, x, xc, rc, &acc, ap);
+        gs_row<ZERO, false, false, false, STN>(A, id, c, r, x, xc, rc);
     }
     if (half == 0) __syncthreads();
   }
-  if (DOT) rz_finish(rz, acc);
 }
 
 // The last class of a forward sweep fused with the first class of the
@@ -747,31 +672,25 @@ __device__ __forceinline__ void gs_lines(const LevelMat<VT> &A, const ClassInfo 
 // lines carry every dependency; the matrix rows of the class are read from
 // DRAM once instead of twice (colour 6's rows come back from L2 in the last
 // phase).
-// DOT: colours 7 and 6 are final after their backward updates (phases 2, 3).
 template <int MODE, class VT, class T, class RT>
 __device__ __forceinline__ void gs_lines_sym3(const LevelMat<VT> &A, const ClassInfo &C, int j0,
-                                              int j1, const RT *__restrict__ r, T *x,
-                                              const RzFuse &rz) {
-  constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0, STN = (MODE & GS_STENCIL) != 0,
-                 DOT = (MODE & GS_DOT) != 0, VEC = (MODE & GS_VEC) != 0;
-  RzAcc acc;
-  const double *ap = (DOT && rz.flex && rz.st->k > 1) ? rz.Ap : nullptr;
+                                              int j1, const RT *__restrict__ r, T *x) {
+  constexpr bool ZERO = (MODE & GS_ZERO_GUESS) != 0, STN = (MODE & GS_STENCIL) != 0;
   const int cnt0 = (j1 - j0) * C.len[0], cnt1 = (j1 - j0) * C.len[1];
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
-    gs_row<ZERO, false, false, false, STN, false, VEC>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r,
-                                                       x, (const T *)nullptr, (T *)nullptr);
+    gs_row<ZERO, false, false, false, STN>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x,
+                                           (const T *)nullptr, (T *)nullptr);
   __syncthreads();
   for (int t = threadIdx.x; t < cnt1; t += blockDim.x)
-    gs_row<ZERO, false, false, true, STN, DOT, VEC>(A, row_of(C, A.nx, A.ny, 1, j0, t), 7, r, x,
-                                                    (const T *)nullptr, (T *)nullptr, &acc, ap);
+    gs_row<ZERO, false, false, true, STN>(A, row_of(C, A.nx, A.ny, 1, j0, t), 7, r, x,
+                                          (const T *)nullptr, (T *)nullptr);
   __syncthreads();
   // Colour 6 backward multiplies every slot; after a zero-guess forward part,
   // rows of colours 6 and 7 in other blocks may still be unwritten, which the
   // exact columns of slots without a neighbour never reach.
   for (int t = threadIdx.x; t < cnt0; t += blockDim.x)
-    gs_row<false, false, false, false, STN, DOT, VEC>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x,
-                                                      (const T *)nullptr, (T *)nullptr, &acc, ap);
-  if (DOT) rz_finish(rz, acc);
+    gs_row<false, false, false, false, STN>(A, row_of(C, A.nx, A.ny, 0, j0, t), 6, r, x,
+                                            (const T *)nullptr, (T *)nullptr);
 }
 
 // A half sweep over one class, lpb lines per block.  MODE bits:
@@ -782,32 +701,27 @@ __device__ __forceinline__ void gs_lines_sym3(const LevelMat<VT> &A, const Class
 // 256-thread blocks per SM; the BF16 sweeps read 2 B per slot and are latency
 // bound, so they are held to 64 registers for four blocks per SM (five,
 // at 48 registers, spill and run slower).
-// The GS_DOT launches (four per V-cycle) keep two FP64 sums per thread and
-// run at three blocks per SM rather than spill.
-template <class VT, int MODE = 0>
-constexpr int gs_min_blocks() {
-  return std::is_same<VT, uint16_t>::value ? ((MODE & GS_DOT) ? 3 : 4) : 2;
-}
+template <class VT>
+constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 4 : 2; }
 
 template <int MODE, int DIR, int QS, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT, MODE>())
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
 k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done,
-           RzFuse rz) {
+           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
   if (done && *done) return;
   const int j0 = blockIdx.x * lpb;
   const int j1 = min(j0 + lpb, C.lines);
-  gs_lines<MODE, QS, DIR>(A, C, j0, j1, r, x, xc, rc, rz);
+  gs_lines<MODE, QS, DIR>(A, C, j0, j1, r, x, xc, rc);
 }
 
 template <int MODE, class VT, class T, class RT>
-__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT, MODE>())
+__global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
 k_gs_class3_sym(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-                const int *__restrict__ done, RzFuse rz) {
+                const int *__restrict__ done) {
   if (done && *done) return;
   const int j0 = blockIdx.x * lpb;
   const int j1 = min(j0 + lpb, C.lines);
-  gs_lines_sym3<MODE>(A, C, j0, j1, r, x, rz);
+  gs_lines_sym3<MODE>(A, C, j0, j1, r, x);
 }
 
 // Residual restricted at the injected points (colour 0: even ix, iy, iz):
@@ -1476,87 +1390,57 @@ struct ValsOf<float> {
 };
 
 // The class kernels.  EXTRA: GS_STENCIL (FP64: columns from the stencil
-// offsets) or GS_VEC (FP32 x: paired x gathers), added to every launch's mode.
+// offsets), added to every launch's mode.
 template <int EXTRA, class T, class RT>
 int launch_gs_rows(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                   const T *xc, T *rc, const int *done, cudaStream_t s, const RzFuse *rzp) {
+                   const T *xc, T *rc, const int *done, cudaStream_t s) {
   using VT = typename ValsOf<T>::VT;
   const LevelMat<VT> A = mat_of(L, ValsOf<T>::get(L));
   const dim3 g(L.blocks[q]), b(L.threads[q]);
   const int lpb = L.lines_per_block[q];
   const ClassInfo &C = L.cls[q];
-  const RzFuse rz = rzp ? *rzp : RzFuse();
-  if (mode & GS_DOT) {
-    // the mixed V-cycle's last four finest-level launches (no FP64 variants)
-    if constexpr (std::is_same<T, float>::value) {
-      if (!rzp) return 0;
-      if (mode == (GS_SYM3 | GS_DOT) && q == 3) {
-        k_gs_class3_sym<GS_DOT | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done, rz);
-        return 1;
-      }
-      if (mode == (GS_PLAIN | GS_DOT) && backward) {
-        k_gs_class<GS_DOT | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
-        return 1;
-      }
-    }
-    return 0;
-  }
   if (mode & GS_SYM3) {
     if (q != 3) return 0;
     if (mode & GS_ZERO_GUESS)
-      k_gs_class3_sym<GS_ZERO_GUESS | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done, rz);
+      k_gs_class3_sym<GS_ZERO_GUESS | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done);
     else
-      k_gs_class3_sym<GS_PLAIN | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done, rz);
+      k_gs_class3_sym<GS_PLAIN | EXTRA><<<g, b, 0, s>>>(A, C, lpb, r, x, done);
     return 1;
   }
   if (mode == GS_ZERO_GUESS && !backward) {
     switch (q) {
-      case 0: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
-      case 1: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
-      case 2: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 2><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
-      default: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 3><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz); break;
+      case 0: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      case 1: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      case 2: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 2><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      default: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 3><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
     }
     return 1;
   }
   if (mode == GS_RESTRICT && backward && q == 0) {
-    k_gs_class<GS_RESTRICT | EXTRA, 1, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
+    k_gs_class<GS_RESTRICT | EXTRA, 1, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
     return 1;
   }
   if (mode == GS_PROLONG && !backward && q == 0) {
-    k_gs_class<GS_PROLONG | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
+    k_gs_class<GS_PROLONG | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
     return 1;
   }
   if (mode != GS_PLAIN) return 0;
   if (backward)
-    k_gs_class<GS_PLAIN | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
+    k_gs_class<GS_PLAIN | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
   else
-    k_gs_class<GS_PLAIN | EXTRA, 0, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done, rz);
+    k_gs_class<GS_PLAIN | EXTRA, 0, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
   return 1;
-}
-
-// HPCGX_VEC_GATHER=0 keeps the one-load-per-neighbour gathers of the mixed
-// sweeps (the paired gathers are the default where they apply).
-bool vec_gathers_enabled() {
-  static const bool on = [] {
-    const char *e = std::getenv("HPCGX_VEC_GATHER");
-    return !(e && e[0] == '0');
-  }();
-  return on;
 }
 
 template <class T, class RT>
 int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                    const T *xc, T *rc, const int *done, cudaStream_t s, const RzFuse *rz) {
+                    const T *xc, T *rc, const int *done, cudaStream_t s) {
   if (L.blocks[q] == 0) return 0;
   if constexpr (std::is_same<T, double>::value) {
     if (L.stencil_cols)
-      return launch_gs_rows<GS_STENCIL>(L, q, backward, mode, r, x, xc, rc, done, s, rz);
-  } else {
-    // paired gathers: x-lines start on even rows and x is 8-byte aligned
-    if (vec_gathers_enabled() && L.nx % 2 == 0 && ((uintptr_t)x & 7) == 0)
-      return launch_gs_rows<GS_VEC>(L, q, backward, mode, r, x, xc, rc, done, s, rz);
+      return launch_gs_rows<GS_STENCIL>(L, q, backward, mode, r, x, xc, rc, done, s);
   }
-  return launch_gs_rows<0>(L, q, backward, mode, r, x, xc, rc, done, s, rz);
+  return launch_gs_rows<0>(L, q, backward, mode, r, x, xc, rc, done, s);
 }
 
 template <class T, class RT>
@@ -1618,13 +1502,13 @@ int launch_rank_sum(int nranks, double *const *bufs, int count, cudaStream_t s) 
 
 template int launch_gs_class<double, double>(const LevelDev &, int, int, int, const double *,
                                              double *, const double *, double *, const int *,
-                                             cudaStream_t, const RzFuse *);
+                                             cudaStream_t);
 template int launch_gs_class<float, double>(const LevelDev &, int, int, int, const double *,
                                             float *, const float *, float *, const int *,
-                                            cudaStream_t, const RzFuse *);
+                                            cudaStream_t);
 template int launch_gs_class<float, float>(const LevelDev &, int, int, int, const float *,
                                            float *, const float *, float *, const int *,
-                                           cudaStream_t, const RzFuse *);
+                                           cudaStream_t);
 
 int launch_waxpby(int64_t n, double alpha, const double *x, double beta, const double *y,
                   double *w, const int *done, cudaStream_t s) {

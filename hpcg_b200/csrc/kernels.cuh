@@ -73,30 +73,9 @@ enum GsMode : int {
   GS_RESTRICT = 2,
   GS_PROLONG = 4,
   GS_SYM3 = 8,
-  // GS_DOT: one of the four launches that write the finest level's final
-  // correction z (the post-smoother's class 3 forward+backward and backward
-  // classes 2, 1, 0) also takes CG's r.z and, for the flexible solver,
-  // z.Ap_{k-1} over the rows it finalises (mixed V-cycle only)
-  GS_DOT = 16,
   // internal to the kernels: the FP64 sweeps derive their columns from the
   // stencil offsets (LevelDev::stencil_cols)
-  GS_STENCIL = 32,
-  // internal to the kernels: the mixed sweeps' x gathers take the aligned
-  // pair of a row's three x-neighbours on a line in one 8-byte load
-  GS_VEC = 64
-};
-
-// The r.z reduction of src/CG.cpp:109-112 spread over the four GS_DOT
-// launches: each reduces its rows deterministically; launches 0-2 store their
-// totals in part, launch 3 adds the four totals in launch order and runs
-// CG's beta step (FIN_CG_RZ) -- or defers it on a sharded problem.
-struct RzFuse {
-  Reduce red;
-  double *part = nullptr;     // 3 x 2 totals
-  CgState *st = nullptr;
-  const double *Ap = nullptr; // A p of the previous iteration (flexible solver)
-  int slot = 0;               // 0..3
-  int flex = 0;
+  GS_STENCIL = 32
 };
 
 // Layout / set-up ---------------------------------------------------------
@@ -121,8 +100,7 @@ int launch_spmv32(const LevelDev &L, const float *x, float *y, cudaStream_t s);
 // vectors) or float (BF16 values, FP32 vectors); RT is the right-hand side type.
 template <class T, class RT>
 int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                     const T *xc, T *rc, const int *done, cudaStream_t s,
-                     const RzFuse *rz = nullptr);
+                     const T *xc, T *rc, const int *done, cudaStream_t s);
 
 
 // Vectors -----------------------------------------------------------------

@@ -145,7 +145,6 @@ struct hpcgx_problem {
   double *tmp = nullptr;      // staging for host diagonals
   double *stage[3] = {};      // staging of the host-buffer operators (allocated on first use)
   double *result = nullptr;   // device scalars of standalone reductions
-  double *rz_part = nullptr;  // totals of the first three GS_DOT launches (3 x 2)
   CgState *st = nullptr;
   Reduce red;
   // graphs of one CG iteration
@@ -264,9 +263,9 @@ struct hpcgx_problem {
   // ---- multigrid
   template <class T, class RT0>
   int gs_launch(int l, int q, int backward, int mode, const void *r, T *x, const T *xc, T *rc,
-                const int *done, const RzFuse *rz = nullptr) {
+                const int *done) {
     const bool mixed = std::is_same<T, float>::value;
-    const int sweep = mode & ~GS_DOT;
+    const int sweep = mode;
     int kinds = 0;
     if (l == 0) {
       kinds |= HPCGX_PROBE_GS_FINE;
@@ -275,27 +274,20 @@ struct hpcgx_problem {
     double bytes = 0.0;
     if ((kinds & probe) || capturing) {
       bytes = gs_bytes(l, q, sweep, mixed);
-      // GS_DOT reads A p of the previous iteration for the rows it finalises
-      // (all but the first iteration; counted for every one)
-      if ((mode & GS_DOT) && rz && rz->flex)
-        bytes += 8.0 * (double)(L[l].ccount[2 * q] + L[l].ccount[2 * q + 1]);
     }
     return probed(kinds, bytes, [&]() {
       if (l == 0)
         return launch_gs_class<T, RT0>(L[l], q, backward, mode, static_cast<const RT0 *>(r), x,
-                                       xc, rc, done, stream, rz);
+                                       xc, rc, done, stream);
       return launch_gs_class<T, T>(L[l], q, backward, mode, static_cast<const T *>(r), x, xc,
-                                   rc, done, stream, rz);
+                                   rc, done, stream);
     });
   }
 
   // One V-cycle (src/ComputeMG_ref.cpp:39-63) with all levels fused as
-  // described in kernels.cu.  r0 / x0 are the finest level's vectors.  With
-  // rz, the four launches that finalise x0 (the finest post-smoother's class 3
-  // forward+backward and backward classes 2, 1, 0) also take CG's r.z
-  // (GS_DOT, slots 0..3); the caller checked that they can (rz_fusable).
+  // described in kernels.cu.  r0 / x0 are the finest level's vectors.
   template <class T, class RT0>
-  int vcycle(const RT0 *r0, T *x0, const int *done, const RzFuse *rz = nullptr) {
+  int vcycle(const RT0 *r0, T *x0, const int *done) {
     const void *rl[kMaxLevels];
     T *xl[kMaxLevels];
     for (int l = 0; l < nlev; ++l) {
@@ -327,37 +319,11 @@ struct hpcgx_problem {
       for (int q = 0; q < 3; ++q)
         TRY((gs_launch<T, RT0>(l, q, 0, q == 0 ? GS_PROLONG : GS_PLAIN, rl[l], xl[l],
                                lvl_x(L[l + 1], (T *)nullptr), nullptr, done)));
-      RzFuse f[4];
-      const bool dot = rz && l == 0;
-      for (int i = 0; dot && i < 4; ++i) {
-        f[i] = *rz;
-        f[i].slot = i;
-      }
-      TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3 | (dot ? GS_DOT : 0), rl[l], xl[l], nullptr,
-                             nullptr, done, dot ? &f[0] : nullptr)));
+      TRY((gs_launch<T, RT0>(l, 3, 0, GS_SYM3, rl[l], xl[l], nullptr, nullptr, done)));
       for (int q = 2; q >= 0; --q)
-        TRY((gs_launch<T, RT0>(l, q, 1, GS_PLAIN | (dot ? GS_DOT : 0), rl[l], xl[l], nullptr,
-                               nullptr, done, dot ? &f[3 - q] : nullptr)));
+        TRY((gs_launch<T, RT0>(l, q, 1, GS_PLAIN, rl[l], xl[l], nullptr, nullptr, done)));
     }
     return HPCGX_OK;
-  }
-
-  // The mixed solver's r.z rides on its V-cycle's last four launches when the
-  // V-cycle has a coarse level (so that those launches are the finest
-  // post-smoother's); HPCGX_FUSE_RZ=0 keeps k_cg_rz.  The sharded solver
-  // defers the totals to the sum over the ranks, as k_cg_rz's.
-  bool rz_fusable() const {
-    static const bool on = env_int("HPCGX_FUSE_RZ", 1) != 0;
-    return on && nlev >= 2 && rz_part;
-  }
-  RzFuse rz_fuse(bool defer = false) const {
-    RzFuse f;
-    f.red = defer ? deferred() : red;
-    f.part = rz_part;
-    f.st = st;
-    f.Ap = Ap;
-    f.flex = 1;
-    return f;
   }
 
   template <class T, class RT>
@@ -408,9 +374,6 @@ struct hpcgx_problem {
       note(launch_copy_z(n, r, z, st, stream));
     } else if (kind == G_FP64_PREC) {
       TRY((vcycle<double, double>(r, z, done)));
-    } else if (rz_fusable()) {
-      const RzFuse f = rz_fuse();
-      TRY((vcycle<float, double>(r, z32, done, &f)));
     } else {
       TRY((vcycle<float, double>(r, z32, done)));
     }
@@ -423,12 +386,9 @@ struct hpcgx_problem {
     };
     if (kind == G_FP64_NOPREC) vec_bytes(16.0);
     if (kind == G_MIXED) {
-      // r.z and z.Ap_{k-1} (src/CG.cpp:109-112): taken by the V-cycle's last
-      // launches when they can, else here
-      if (!rz_fusable()) {
-        note(launch_cg_rz<float>(n, r, z32, Ap, red, st, stream));
-        vec_bytes(20.0);
-      }
+      // r.z and z.Ap_{k-1} (src/CG.cpp:109-112)
+      note(launch_cg_rz<float>(n, r, z32, Ap, red, st, stream));
+      vec_bytes(20.0);
       note(launch_cg_p<float>(n, z32, p, st, stream));
       vec_bytes(20.0);
     } else {
@@ -635,31 +595,8 @@ struct hpcgx_problem {
   // rc: the last backward class forms the restricted residual (GS_RESTRICT).
   template <class T, class RT>
   void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done,
-                   const T *xc = nullptr, T *rc = nullptr, const RzFuse *rz = nullptr) {
+                   const T *xc = nullptr, T *rc = nullptr) {
     const int m0 = zero ? GS_ZERO_GUESS : GS_PLAIN;
-    if (rz) {   // the finest post-smoother of the mixed solver: GS_DOT, slots 0..3
-      for (int q = 0; q < 3; ++q) {
-        const int m = (q == 0 && xc) ? GS_PROLONG : m0;
-        add(pl, [=]() {
-          note(launch_gs_class<T, RT>(L[l], q, 0, m, r, x, xc, nullptr, done, stream));
-          return HPCGX_OK;
-        });
-      }
-      for (int i = 0; i < 4; ++i) {
-        RzFuse f = *rz;
-        f.slot = i;
-        const int q = i == 0 ? 3 : 3 - i;
-        const int m = (i == 0 ? GS_SYM3 : GS_PLAIN) | GS_DOT;
-        add(pl, [=]() {
-          const int k = launch_gs_class<T, RT>(L[l], q, i == 0 ? 0 : 1, m, r, x, nullptr, nullptr,
-                                               done, stream, &f);
-          if (!k) return fail(HPCGX_ESTATE, "the fused r.z sweep is not available here");
-          note(k);
-          return HPCGX_OK;
-        });
-      }
-      return;
-    }
     for (int q = 0; q < 3; ++q) {
       const int m = (q == 0 && xc) ? GS_PROLONG : m0;
       add(pl, [=]() {
@@ -691,7 +628,7 @@ struct hpcgx_problem {
   // correction (which the fused prolongation then skips).  x0 must be a
   // haloed vector.
   template <class T, class RT0>
-  void plan_vcycle(Plan &pl, const RT0 *r0, T *x0, const int *done, const RzFuse *rz = nullptr) {
+  void plan_vcycle(Plan &pl, const RT0 *r0, T *x0, const int *done) {
     T *xl[kMaxLevels];
     for (int l = 0; l < nlev; ++l) xl[l] = l == 0 ? x0 : lvl_x(L[l], (T *)nullptr);
     auto rl = [&](int l) { return lvl_r(L[l], (T *)nullptr); };
@@ -739,7 +676,7 @@ struct hpcgx_problem {
       });
       add_halo(pl, l, x, sizeof(T));
       if (l == 0)
-        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc, nullptr, rz);
+        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc);
       else
         plan_sweeps<T, T>(pl, l, rl(l), x, false, done, xc);
     }
@@ -817,22 +754,15 @@ struct hpcgx_problem {
     else if (kind == G_FP64_PREC)
       plan_vcycle<double, double>(pl, r, z, done);
     const bool mixed = kind == G_MIXED;
-    // the mixed solver's r.z inside its V-cycle (as the graph solver's), else
-    // a separate reduction; either way the totals are deferred to the sum
-    const bool fused = mixed && rz_fusable();
-    if (mixed) {
-      const RzFuse f = rz_fuse(true);
-      plan_vcycle<float, double>(pl, r, z32, done, fused ? &f : nullptr);
-    }
-    if (!fused)
-      add(pl, [=]() {
-        if (mixed) {
-          note(launch_cg_rz<float>(n, r, z32, Ap, deferred(), st, stream));
-        } else {
-          note(launch_cg_rz<double>(n, r, z, nullptr, deferred(), st, stream));
-        }
-        return HPCGX_OK;
-      });
+    if (mixed) plan_vcycle<float, double>(pl, r, z32, done);
+    add(pl, [=]() {
+      if (mixed) {
+        note(launch_cg_rz<float>(n, r, z32, Ap, deferred(), st, stream));
+      } else {
+        note(launch_cg_rz<double>(n, r, z, nullptr, deferred(), st, stream));
+      }
+      return HPCGX_OK;
+    });
     add_sum(pl, FIN_CG_RZ, mixed ? 2 : 1);
     add(pl, [=]() {
       if (mixed)
@@ -881,8 +811,7 @@ hpcgx_problem::~hpcgx_problem() {
   for (double *ptr : stage) cudaFree(ptr);
   for (void *ptr : halo_bases) cudaFree(ptr);
   for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)Ap, (void *)tmp, (void *)result,
-                    (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter,
-                    (void *)rz_part})
+                    (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter})
     cudaFree(ptr);
   if (gen) general_destroy(gen);
   if (own_stream) cudaStreamDestroy(own_stream);
@@ -1468,7 +1397,6 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   if ((rc = p->alloc_halo((void **)&p->z32, n, sizeof(float), plane0))) return bail(rc);
   if ((rc = p->alloc((void **)&p->gsum, 2 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->result, 4 * sizeof(double)))) return bail(rc);
-  if ((rc = p->alloc((void **)&p->rz_part, 6 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->st, sizeof(CgState)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->red.partials, red_cap * sizeof(double)))) return bail(rc);
   const int64_t ncounters = 1 + (red_cap + 1023) / 1024;   // top counter + one per group
