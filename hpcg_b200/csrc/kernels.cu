@@ -924,20 +924,42 @@ k_cg_rz(int64_t n, const double *__restrict__ r, const ZT *__restrict__ z,
 }
 
 // p = z (k == 1) or p = z + beta p (WAXPBY(1, z, beta, p), src/CG.cpp:115).
+// With x given, the previous iteration's x += alpha p (src/CG.cpp:121) is
+// applied here, while p_{k-1} is read anyway, instead of in k_cg_xr: the same
+// operation on the same operands, one read of p fewer per iteration.
+// k_cg_xflush applies the last iteration's update after the loop.
 template <class ZT>
 __global__ void __launch_bounds__(kThreads)
-k_cg_p(int64_t n, const ZT *__restrict__ z, double *p, const CgState *__restrict__ st) {
+k_cg_p(int64_t n, const ZT *__restrict__ z, double *p, const CgState *__restrict__ st,
+       double *x) {
   if (st->done) return;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const bool first = st->k == 1;
-  const double beta = st->beta;
+  const double beta = st->beta, alpha = st->alpha;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     const double zi = (double)z[i];
-    p[i] = first ? zi : rn_add(zi, rn_mul(beta, p[i]));
+    if (first) {
+      p[i] = zi;
+    } else {
+      const double pi = p[i];
+      if (x) x[i] = rn_add(x[i], rn_mul(alpha, pi));
+      p[i] = rn_add(zi, rn_mul(beta, pi));
+    }
   }
 }
 
-// x += alpha p; r -= alpha Ap; |r|^2 (src/CG.cpp:121-124).
+// The deferred x += alpha p of the last iteration that ran.
+__global__ void __launch_bounds__(kThreads)
+k_cg_xflush(int64_t n, const double *__restrict__ p, double *x, const CgState *__restrict__ st) {
+  if (st->niters < 1) return;
+  const double alpha = st->alpha;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = rn_add(x[i], rn_mul(alpha, p[i]));
+}
+
+// x += alpha p (unless deferred: x null); r -= alpha Ap; |r|^2
+// (src/CG.cpp:121-124).
 __global__ void __launch_bounds__(kThreads)
 k_cg_xr(int64_t n, const double *__restrict__ p, const double *__restrict__ Ap, double *x,
         double *r, Reduce red, CgState *st) {
@@ -946,7 +968,7 @@ k_cg_xr(int64_t n, const double *__restrict__ p, const double *__restrict__ Ap, 
   const double alpha = st->alpha, malpha = -st->alpha;
   double acc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
-    x[i] = rn_add(x[i], rn_mul(alpha, p[i]));
+    if (x) x[i] = rn_add(x[i], rn_mul(alpha, p[i]));
     const double ri = rn_add(r[i], rn_mul(malpha, Ap[i]));
     r[i] = ri;
     acc += ri * ri;
@@ -1583,12 +1605,19 @@ template int launch_cg_rz<float>(int64_t, const double *, const float *, const d
                                  const Reduce &, CgState *, cudaStream_t);
 
 template <class ZT>
-int launch_cg_p(int64_t n, const ZT *z, double *p, CgState *st, cudaStream_t s) {
-  k_cg_p<ZT><<<vector_blocks(n), kThreads, 0, s>>>(n, z, p, st);
+int launch_cg_p(int64_t n, const ZT *z, double *p, CgState *st, cudaStream_t s, double *x) {
+  k_cg_p<ZT><<<vector_blocks(n), kThreads, 0, s>>>(n, z, p, st, x);
   return 1;
 }
-template int launch_cg_p<double>(int64_t, const double *, double *, CgState *, cudaStream_t);
-template int launch_cg_p<float>(int64_t, const float *, double *, CgState *, cudaStream_t);
+template int launch_cg_p<double>(int64_t, const double *, double *, CgState *, cudaStream_t,
+                                 double *);
+template int launch_cg_p<float>(int64_t, const float *, double *, CgState *, cudaStream_t,
+                                double *);
+
+int launch_cg_xflush(int64_t n, const double *p, double *x, const CgState *st, cudaStream_t s) {
+  k_cg_xflush<<<vector_blocks(n), kThreads, 0, s>>>(n, p, x, st);
+  return 1;
+}
 
 int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r,
                  const Reduce &red, CgState *st, cudaStream_t s) {

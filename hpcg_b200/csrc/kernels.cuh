@@ -149,7 +149,9 @@ template <class ZT>
 int launch_cg_rz(int64_t n, const double *r, const ZT *z, const double *Ap, const Reduce &red,
                   CgState *st, cudaStream_t s);
 template <class ZT>
-int launch_cg_p(int64_t n, const ZT *z, double *p, CgState *st, cudaStream_t s);
+int launch_cg_p(int64_t n, const ZT *z, double *p, CgState *st, cudaStream_t s,
+                double *x = nullptr);
+int launch_cg_xflush(int64_t n, const double *p, double *x, const CgState *st, cudaStream_t s);
 int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r,
                   const Reduce &red, CgState *st, cudaStream_t s);
 int launch_copy_z(int64_t n, const double *r, double *z, const CgState *st, cudaStream_t s);

@@ -209,7 +209,9 @@ struct hpcgx_problem {
   double gs_bytes(int l, int q, int mode, bool mixed) const {
     const LevelDev &A = L[l];
     // mixed: BF16 value per slot, columns derived from the stencil offsets
-    const double vb = mixed ? 2.0 : 8.0, cb = mixed ? 0.0 : 4.0, xb = mixed ? 4.0 : 8.0;
+    // (FP64 with stencil columns: no column reads either)
+    const double vb = mixed ? 2.0 : 8.0, cb = (mixed || A.stencil_cols) ? 0.0 : 4.0;
+    const double xb = mixed ? 4.0 : 8.0;
     const double rb = (mixed && l > 0) ? 4.0 : 8.0;
     double total = 0.0;
     for (int px = 0; px < 2; ++px) {
@@ -379,8 +381,9 @@ struct hpcgx_problem {
     }
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][1], stream, cudaEventRecordExternal));
     // vector kernels, bytes per row: r.z reads r, z (and Ap); p = z + beta p
-    // reads z and p and writes p; x += alpha p, r -= alpha Ap reads p, Ap and
-    // reads and writes x and r
+    // reads z and p and writes p, and applies the previous iteration's
+    // x += alpha p (reads and writes x); r -= alpha Ap reads Ap and reads and
+    // writes r
     auto vec_bytes = [&](double per_row) {
       if (capturing) graph_bytes[kind] += per_row * (double)n;
     };
@@ -389,12 +392,12 @@ struct hpcgx_problem {
       // r.z and z.Ap_{k-1} (src/CG.cpp:109-112)
       note(launch_cg_rz<float>(n, r, z32, Ap, red, st, stream));
       vec_bytes(20.0);
-      note(launch_cg_p<float>(n, z32, p, st, stream));
-      vec_bytes(20.0);
+      note(launch_cg_p<float>(n, z32, p, st, stream, x));
+      vec_bytes(20.0 + 16.0);
     } else {
       note(launch_cg_rz<double>(n, r, z, nullptr, red, st, stream));
-      note(launch_cg_p<double>(n, z, p, st, stream));
-      vec_bytes(16.0 + 24.0);
+      note(launch_cg_p<double>(n, z, p, st, stream, x));
+      vec_bytes(16.0 + 24.0 + 16.0);
     }
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][2], stream, cudaEventRecordExternal));
     // The mixed solver's FP64 SpMV derives its columns from the stencil
@@ -419,8 +422,8 @@ struct hpcgx_problem {
       return launch_spmv(L[0], p, Ap, &red, FIN_CG_PAP, st, done, stream, implicit_cols);
     }));
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][3], stream, cudaEventRecordExternal));
-    note(launch_cg_xr(n, p, Ap, x, r, red, st, stream));
-    vec_bytes(48.0);
+    note(launch_cg_xr(n, p, Ap, nullptr, r, red, st, stream));
+    vec_bytes(24.0);
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][4], stream, cudaEventRecordExternal));
     return HPCGX_OK;
   }
@@ -533,6 +536,8 @@ struct hpcgx_problem {
       // still a result (src/CG.cpp:89-96 sets normr and normr0 before the loop)
       CK(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, stream));
     }
+    // the last iteration's x += alpha p, deferred by k_cg_p
+    note(launch_cg_xflush(n, p, x, st, stream));
     if (xu != x) CK(cudaMemcpyAsync(xu, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     CK(cudaStreamSynchronize(stream));
     if (niters) *niters = h.niters;
@@ -766,9 +771,9 @@ struct hpcgx_problem {
     add_sum(pl, FIN_CG_RZ, mixed ? 2 : 1);
     add(pl, [=]() {
       if (mixed)
-        note(launch_cg_p<float>(n, z32, p, st, stream));
+        note(launch_cg_p<float>(n, z32, p, st, stream, x));
       else
-        note(launch_cg_p<double>(n, z, p, st, stream));
+        note(launch_cg_p<double>(n, z, p, st, stream, x));
       return HPCGX_OK;
     });
     add_halo(pl, 0, p, sizeof(double));
@@ -779,7 +784,7 @@ struct hpcgx_problem {
     });
     add_sum(pl, FIN_CG_PAP, 1);
     add(pl, [=]() {
-      note(launch_cg_xr(n, p, Ap, x, r, deferred(), st, stream));
+      note(launch_cg_xr(n, p, Ap, nullptr, r, deferred(), st, stream));
       return HPCGX_OK;
     });
     add_sum(pl, FIN_CG_RR, 1);
@@ -862,92 +867,146 @@ void parallel_for(int64_t n, F f) {
   for (auto &th : ts) th.join();
 }
 
+// Natural row of storage row k, or -1 for a row that only pads a colour to a
+// multiple of 32 (the inverse of storage_row_host).
+int64_t natural_row_host(const LevelDev &A, int64_t k) {
+  for (int c = 0; c < 8; ++c) {
+    if (k < A.cstart[c] || k >= A.cstart[c] + A.ccount[c]) continue;
+    const int px = c & 1, q = c >> 1;
+    const int64_t off = k - A.cstart[c], len = A.cls[q].len[px];
+    const int64_t j = off / len, ix = 2 * (off % len) + px;
+    const int64_t iy = 2 * (j % A.cls[q].nyq) + (q & 1), iz = 2 * (j / A.cls[q].nyq) + (q >> 1);
+    return ix + A.nx * (iy + (int64_t)A.ny * iz);
+  }
+  return -1;
+}
+
+// Pinned host staging of one chunk of 32-row slices, and the event that marks
+// the end of its last copy to the device.
+struct PinnedChunk {
+  double *vals = nullptr;
+  int32_t *cols = nullptr;
+  cudaEvent_t copied = nullptr;
+  bool pending = false;
+  ~PinnedChunk() {
+    if (copied) {
+      if (pending) cudaEventSynchronize(copied);
+      cudaEventDestroy(copied);
+    }
+    if (vals) cudaFreeHost(vals);
+    if (cols) cudaFreeHost(cols);
+  }
+};
+
 // Shared body of the two host loaders: get(i, j, col, val) yields entry j of
-// row i.  Rows are validated and scattered into the device layout in
-// parallel; the first failing row (lowest index) is reported.
+// row i.  The level is filled in chunks of 4096 slices in storage order: the
+// host's cores validate and scatter the rows of one chunk into pinned
+// staging while the previous chunk is copied to the device.  On a malformed
+// row the load stops, the level is left unloaded, and the failing row with
+// the lowest index is reported.
 template <class Nnz, class Get>
 int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
   TRY(check_level(p, level));
   LevelDev &A = p->L[level];
-  const size_t slots = (size_t)A.storage_rows * HPCGX_STENCIL;
-  std::unique_ptr<double[]> vals(new double[slots]);
-  std::unique_ptr<int32_t[]> cols(new int32_t[slots]);
-  // rows that only pad a colour to 32 rows: value 0, column 0
-  for (int c = 0; c < 8; ++c) {
-    const int64_t end = (c < 7 ? A.cstart[c + 1] : A.storage_rows);
-    for (int64_t k = A.cstart[c] + A.ccount[c]; k < end; ++k)
-      for (int s = 0; s < HPCGX_STENCIL; ++s) {
-        vals[vidx(k, s)] = 0.0;
-        cols[cidx(k, s)] = 0;
-      }
-  }
-  struct Err {
-    int64_t row = -1;
-    std::string msg;
-  };
-  std::vector<Err> errs(64);
-  parallel_for(A.n, [&](int64_t r0, int64_t r1, int t) {
-    for (int64_t row = r0; row < r1; ++row) {
-      const int ix = (int)(row % A.nx), iy = (int)((row / A.nx) % A.ny),
-                iz = (int)(row / ((int64_t)A.nx * A.ny));
-      const int64_t k = storage_row_host(A, row);
-      for (int s = 0; s < HPCGX_STENCIL; ++s) {
-        vals[vidx(k, s)] = 0.0;
-        cols[cidx(k, s)] = (int32_t)row;
-      }
-      auto bad = [&](const std::string &m) {
-        errs[t].row = row;
-        errs[t].msg = "row " + std::to_string(row) + ": " + m;
-      };
-      const int nz = nnz_of(row);
-      if (nz < 1 || nz > HPCGX_STENCIL) {
-        bad(std::to_string(nz) + " entries");
-        return;
-      }
-      int last = -1;
-      bool diag = false;
-      for (int j = 0; j < nz; ++j) {
-        int32_t col;
-        double v;
-        get(row, j, col, v);
-        if (col < 0 || col >= A.n) {
-          bad("column out of range");
-          return;
-        }
-        const int jx = col % A.nx, jy = (col / A.nx) % A.ny,
-                  jz = (int)(col / ((int64_t)A.nx * A.ny));
-        const int dx = jx - ix, dy = jy - iy, dz = jz - iz;
-        if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) {
-          bad("column " + std::to_string(col) + " is not a stencil neighbour");
-          return;
-        }
-        const int s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
-        if (s <= last) {
-          bad("entries not in stencil order");
-          return;
-        }
-        last = s;
-        diag |= (s == HPCGX_DIAG_SLOT);
-        vals[vidx(k, s)] = v;
-        cols[cidx(k, s)] = col;
-      }
-      if (!diag) {
-        bad("no diagonal");
-        return;
-      }
+  // One row: validates it and writes its 27 slots through put(s, col, val);
+  // returns an empty string or what is wrong with the row.
+  auto scan_row = [&](int64_t row, auto put) -> std::string {
+    const int ix = (int)(row % A.nx), iy = (int)((row / A.nx) % A.ny),
+              iz = (int)(row / ((int64_t)A.nx * A.ny));
+    for (int s = 0; s < HPCGX_STENCIL; ++s) put(s, (int32_t)row, 0.0);
+    const int nz = nnz_of(row);
+    if (nz < 1 || nz > HPCGX_STENCIL) return std::to_string(nz) + " entries";
+    int last = -1;
+    bool diag = false;
+    for (int j = 0; j < nz; ++j) {
+      int32_t col;
+      double v;
+      get(row, j, col, v);
+      if (col < 0 || col >= A.n) return "column out of range";
+      const int jx = col % A.nx, jy = (col / A.nx) % A.ny,
+                jz = (int)(col / ((int64_t)A.nx * A.ny));
+      const int dx = jx - ix, dy = jy - iy, dz = jz - iz;
+      if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1)
+        return "column " + std::to_string(col) + " is not a stencil neighbour";
+      const int s = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+      if (s <= last) return "entries not in stencil order";
+      last = s;
+      diag |= (s == HPCGX_DIAG_SLOT);
+      put(s, col, v);
     }
-  });
-  const Err *first = nullptr;
-  for (const Err &e : errs)
-    if (e.row >= 0 && (!first || e.row < first->row)) first = &e;
-  if (first) return fail(HPCGX_ELAYOUT, first->msg);
-  CK(cudaMemcpyAsync(A.vals, vals.get(), slots * sizeof(double), cudaMemcpyHostToDevice,
-                     p->stream));
-  CK(cudaMemcpyAsync(A.cols, cols.get(), slots * sizeof(int32_t), cudaMemcpyHostToDevice,
-                     p->stream));
-  CK(cudaStreamSynchronize(p->stream));
-  p->loaded[level] = true;
+    if (!diag) return "no diagonal";
+    return std::string();
+  };
+  p->loaded[level] = false;
   p->mixed_stale = true;
+  constexpr int64_t kChunkSlices = 4096;
+  const int64_t slices = A.storage_rows / HPCGX_SLICE;
+  const int64_t celems = std::min<int64_t>(slices, kChunkSlices) * kSliceElems;
+  PinnedChunk buf[2];
+  for (PinnedChunk &b : buf) {
+    CK(cudaHostAlloc((void **)&b.vals, celems * sizeof(double), cudaHostAllocDefault));
+    CK(cudaHostAlloc((void **)&b.cols, celems * sizeof(int32_t), cudaHostAllocDefault));
+    CK(cudaEventCreateWithFlags(&b.copied, cudaEventDisableTiming));
+  }
+  bool failed = false;
+  std::vector<char> bad(64);
+  for (int64_t c0 = 0, it = 0; c0 < slices && !failed; c0 += kChunkSlices, ++it) {
+    PinnedChunk &b = buf[it & 1];
+    if (b.pending) CK(cudaEventSynchronize(b.copied));
+    b.pending = false;
+    const int64_t c1 = std::min(slices, c0 + kChunkSlices);
+    const int64_t k0 = c0 * HPCGX_SLICE, e0 = c0 * kSliceElems;
+    parallel_for((c1 - c0) * HPCGX_SLICE, [&](int64_t a, int64_t e, int t) {
+      for (int64_t k = k0 + a; k < k0 + e; ++k) {
+        const int64_t row = natural_row_host(A, k);
+        if (row < 0) {   // padding: value 0, column 0
+          for (int s = 0; s < HPCGX_STENCIL; ++s) {
+            b.vals[vidx(k, s) - e0] = 0.0;
+            b.cols[cidx(k, s) - e0] = 0;
+          }
+          continue;
+        }
+        const std::string m = scan_row(row, [&](int s, int32_t col, double v) {
+          b.vals[vidx(k, s) - e0] = v;
+          b.cols[cidx(k, s) - e0] = col;
+        });
+        if (!m.empty()) {
+          bad[t] = 1;
+          return;
+        }
+      }
+    });
+    for (char f : bad) failed |= f != 0;
+    if (failed) break;
+    const size_t ne = (size_t)(c1 - c0) * kSliceElems;
+    CK(cudaMemcpyAsync(A.vals + e0, b.vals, ne * sizeof(double), cudaMemcpyHostToDevice,
+                       p->stream));
+    CK(cudaMemcpyAsync(A.cols + e0, b.cols, ne * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       p->stream));
+    CK(cudaEventRecord(b.copied, p->stream));
+    b.pending = true;
+  }
+  CK(cudaStreamSynchronize(p->stream));
+  for (PinnedChunk &b : buf) b.pending = false;
+  if (failed) {
+    // the lowest failing row: each thread's first in natural order
+    std::vector<int64_t> first(64, -1);
+    std::vector<std::string> msg(64);
+    parallel_for(A.n, [&](int64_t a, int64_t e, int t) {
+      for (int64_t row = a; row < e; ++row) {
+        const std::string m = scan_row(row, [](int, int32_t, double) {});
+        if (!m.empty()) {
+          first[t] = row;
+          msg[t] = m;
+          return;
+        }
+      }
+    });
+    for (int t = 0; t < 64; ++t)
+      if (first[t] >= 0) return fail(HPCGX_ELAYOUT, "row " + std::to_string(first[t]) + ": " + msg[t]);
+    return fail(HPCGX_ELAYOUT, "malformed row");
+  }
+  p->loaded[level] = true;
   return HPCGX_OK;
 }
 
@@ -1286,6 +1345,9 @@ int sharded_cg(const std::vector<hpcgx_problem *> &ps, const Runner &run, int ki
     if (h.done) break;
     TRY(run(iter));
   }
+  // the last iteration's x += alpha p, deferred by k_cg_p
+  for (hpcgx_problem *p : ps)
+    p->note(launch_cg_xflush(p->L[0].n, p->p, p->x, p->st, p->stream));
   for (size_t r = 0; r < P; ++r)
     CK(cudaMemcpyAsync(x[r], ps[r]->x, ps[r]->L[0].n * sizeof(double), cudaMemcpyDeviceToDevice,
                        ps[r]->stream));

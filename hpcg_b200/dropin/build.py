@@ -37,7 +37,12 @@ def build(force: bool = False) -> str | None:
             and all(os.path.getmtime(d) <= os.path.getmtime(BINARY) for d in deps)):
         return BINARY
     os.makedirs(os.path.dirname(BINARY), exist_ok=True)
-    cmd = ["g++", "-O3", "-fno-fast-math", "-ffp-contract=off", "-fopenmp", "-DHPCG_NO_MPI", "-w",
+    # HPCG_CONTIGUOUS_ARRAYS: the reference's own build option (setup/Make.*,
+    # line 101) that allocates each level's rows as one block instead of one
+    # allocation per row; it shortens set-up and is honoured alike by
+    # GenerateProblem.cpp here and the reference's DeleteMatrix.
+    cmd = ["g++", "-O3", "-fno-fast-math", "-ffp-contract=off", "-fopenmp", "-DHPCG_NO_MPI",
+           "-DHPCG_CONTIGUOUS_ARRAYS", "-w",
            "-I", REF, "-I", HERE, "-I", os.path.join(ROOT, "include"), "-o", BINARY,
            *ref_srcs, *ours, lib, "-Wl,-rpath,$ORIGIN/../.."]
     out = subprocess.run(cmd, capture_output=True, text=True)

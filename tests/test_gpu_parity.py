@@ -390,6 +390,33 @@ def test_large_grid_properties():
     assert rt < 1e-9
 
 
+def test_load_in_chunks(oracle):
+    """64^3 loads in three chunks of storage slices: the values land where the
+    device generator puts them, and of two malformed rows in different chunks
+    the lower is reported while the level is left unloaded."""
+    from hpcg_b200 import HPCGXError, Problem
+    L, _, _, _ = oracle.hierarchy(64, 64, 64)
+    P, Q = Problem(64, 64, 64), Problem(64, 64, 64)
+    try:
+        Q.generate("hpcg")
+        P.load_level(0, L[0].nnz, L[0].cols, L[0].vals)
+        v1, c1 = P.get_values(0)
+        v2, c2 = Q.get_values(0)
+        assert torch.equal(v1, v2) and torch.equal(c1, c2)
+        bad = L[0].cols.copy()
+        bad[27 * 250000 + 3] = 7                  # not a neighbour (last chunk)
+        bad[27 * 100003] = -1                     # out of range (first chunk)
+        with pytest.raises(HPCGXError) as e:
+            P.load_level(0, L[0].nnz, bad, L[0].vals)
+        assert e.value.code == 5 and "row 100003:" in str(e.value)
+        with pytest.raises(HPCGXError) as e:
+            P.spmv(torch.ones(P.rows(), dtype=torch.float64, device="cuda"), level=0)
+        assert e.value.code == 3
+    finally:
+        P.close()
+        Q.close()
+
+
 def test_error_paths(oracle):
     from hpcg_b200 import HPCGXError, Problem
     P = Problem(16, 16, 16)
@@ -402,7 +429,7 @@ def test_error_paths(oracle):
     bad[27 * 5] = 4000                            # not a neighbour of row 5
     with pytest.raises(HPCGXError) as e:
         P.load_level(0, L[0].nnz, bad, L[0].vals)
-    assert e.value.code == 5
+    assert e.value.code == 5 and "row 5:" in str(e.value)
     with pytest.raises(HPCGXError) as e:
         P.check_f2c(0, L[0].f2c[::-1].copy())
     assert e.value.code == 5
