@@ -11,6 +11,7 @@ from __future__ import annotations
 import glob
 import os
 import subprocess
+import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
@@ -27,12 +28,14 @@ REPLACED = ["CG.cpp", "ComputeSPMV.cpp", "ComputeSYMGS.cpp", "ComputeMG.cpp",
 def build(force: bool = False) -> str | None:
     if not REF or not os.path.exists(os.path.join(REF, "main.cpp")):
         return None
+    if ROOT not in sys.path:   # run as a script: the package sits two levels up
+        sys.path.insert(0, ROOT)
     from hpcg_b200 import build as hb
     lib = hb.build()
     ref_srcs = sorted(p for p in glob.glob(os.path.join(REF, "*.cpp"))
                       if os.path.basename(p) not in REPLACED)
     ours = sorted(glob.glob(os.path.join(HERE, "*.cpp")))
-    deps = ref_srcs + ours + glob.glob(os.path.join(HERE, "*.hpp")) + [lib]
+    deps = ref_srcs + ours + glob.glob(os.path.join(HERE, "*.hpp")) + [lib, __file__]
     if (not force and os.path.exists(BINARY)
             and all(os.path.getmtime(d) <= os.path.getmtime(BINARY) for d in deps)):
         return BINARY
