@@ -122,6 +122,10 @@ namespace hpcgx {
 int set_error(int code, const char *msg) { return fail(code, msg); }
 }  // namespace hpcgx
 
+// 32-row slices per chunk of the host loaders' pinned staging (2 chunks of
+// 4096 x 864 values and columns: 2 x 42 MB)
+constexpr int64_t kPinnedSlices = 4096;
+
 static int env_int(const char *name, int dflt) {
   const char *e = std::getenv(name);
   return e && *e ? std::atoi(e) : dflt;
@@ -180,6 +184,21 @@ struct hpcgx_problem {
   double *gsum = nullptr;            // this rank's deferred reduction totals
   double *hstage[kMaxLevels] = {};   // haloed FP64 staging of operator inputs
   bool sharded() const { return nranks > 1 || nccl != nullptr || comm_halo != nullptr; }
+  // ---- pinned host staging of the host loaders: two chunks of kPinnedSlices
+  // 32-row slices (values and columns), allocated on the first load
+  double *pin_vals[2] = {};
+  int32_t *pin_cols[2] = {};
+  cudaEvent_t pin_copied[2] = {};
+  int pinned_staging() {
+    if (pin_vals[0]) return HPCGX_OK;
+    const size_t e = (size_t)kPinnedSlices * kSliceElems;
+    for (int h = 0; h < 2; ++h) {
+      CK(cudaHostAlloc((void **)&pin_vals[h], e * sizeof(double), cudaHostAllocDefault));
+      CK(cudaHostAlloc((void **)&pin_cols[h], e * sizeof(int32_t), cudaHostAllocDefault));
+      CK(cudaEventCreateWithFlags(&pin_copied[h], cudaEventDisableTiming));
+    }
+    return HPCGX_OK;
+  }
 
   ~hpcgx_problem();
   int alloc(void **ptr, size_t n) {
@@ -815,6 +834,11 @@ hpcgx_problem::~hpcgx_problem() {
   }
   for (double *ptr : stage) cudaFree(ptr);
   for (void *ptr : halo_bases) cudaFree(ptr);
+  for (int h = 0; h < 2; ++h) {
+    if (pin_copied[h]) cudaEventDestroy(pin_copied[h]);
+    if (pin_vals[h]) cudaFreeHost(pin_vals[h]);
+    if (pin_cols[h]) cudaFreeHost(pin_cols[h]);
+  }
   for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)Ap, (void *)tmp, (void *)result,
                     (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter})
     cudaFree(ptr);
@@ -869,34 +893,21 @@ void parallel_for(int64_t n, F f) {
 
 // Natural row of storage row k, or -1 for a row that only pads a colour to a
 // multiple of 32 (the inverse of storage_row_host).
-int64_t natural_row_host(const LevelDev &A, int64_t k) {
+int64_t natural_row_host(const LevelDev &A, int64_t k, int &ix, int &iy, int &iz) {
   for (int c = 0; c < 8; ++c) {
     if (k < A.cstart[c] || k >= A.cstart[c] + A.ccount[c]) continue;
     const int px = c & 1, q = c >> 1;
     const int64_t off = k - A.cstart[c], len = A.cls[q].len[px];
-    const int64_t j = off / len, ix = 2 * (off % len) + px;
-    const int64_t iy = 2 * (j % A.cls[q].nyq) + (q & 1), iz = 2 * (j / A.cls[q].nyq) + (q >> 1);
+    const int64_t j = off / len;
+    ix = (int)(2 * (off - j * len) + px);
+    const int64_t jz = j / A.cls[q].nyq;
+    iy = (int)(2 * (j - jz * A.cls[q].nyq) + (q & 1));
+    iz = (int)(2 * jz + (q >> 1));
     return ix + A.nx * (iy + (int64_t)A.ny * iz);
   }
   return -1;
 }
 
-// Pinned host staging of one chunk of 32-row slices, and the event that marks
-// the end of its last copy to the device.
-struct PinnedChunk {
-  double *vals = nullptr;
-  int32_t *cols = nullptr;
-  cudaEvent_t copied = nullptr;
-  bool pending = false;
-  ~PinnedChunk() {
-    if (copied) {
-      if (pending) cudaEventSynchronize(copied);
-      cudaEventDestroy(copied);
-    }
-    if (vals) cudaFreeHost(vals);
-    if (cols) cudaFreeHost(cols);
-  }
-};
 
 // Shared body of the two host loaders: get(i, j, col, val) yields entry j of
 // row i.  The level is filled in chunks of 4096 slices in storage order: the
@@ -937,40 +948,66 @@ int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
     if (!diag) return "no diagonal";
     return std::string();
   };
+  // The common case without a division per entry: walk the 27 slots once,
+  // matching each entry's column to the next slot whose neighbour exists.
+  // Columns of existing neighbours are distinct, so this accepts exactly the
+  // rows scan_row accepts; a row it rejects goes to scan_row for the message.
+  int64_t off[HPCGX_STENCIL];
+  for (int s = 0; s < HPCGX_STENCIL; ++s)
+    off[s] = (s % 3 - 1) + (int64_t)A.nx * ((s / 3) % 3 - 1 + (int64_t)A.ny * (s / 9 - 1));
+  auto fast_row = [&](int64_t row, int ix, int iy, int iz, auto put) -> bool {
+    for (int s = 0; s < HPCGX_STENCIL; ++s) put(s, (int32_t)row, 0.0);
+    const int nz = nnz_of(row);
+    if (nz < 1 || nz > HPCGX_STENCIL) return false;
+    const bool okx[3] = {ix > 0, true, ix + 1 < A.nx}, oky[3] = {iy > 0, true, iy + 1 < A.ny},
+               okz[3] = {iz > 0, true, iz + 1 < A.nz};
+    int s = 0;
+    bool diag = false;
+    for (int j = 0; j < nz; ++j) {
+      int32_t col;
+      double v;
+      get(row, j, col, v);
+      for (;; ++s) {
+        if (s == HPCGX_STENCIL) return false;
+        if (okx[s % 3] && oky[(s / 3) % 3] && okz[s / 9] && row + off[s] == col) break;
+      }
+      diag |= (s == HPCGX_DIAG_SLOT);
+      put(s, col, v);
+      ++s;
+    }
+    return diag;
+  };
   p->loaded[level] = false;
   p->mixed_stale = true;
-  constexpr int64_t kChunkSlices = 4096;
   const int64_t slices = A.storage_rows / HPCGX_SLICE;
-  const int64_t celems = std::min<int64_t>(slices, kChunkSlices) * kSliceElems;
-  PinnedChunk buf[2];
-  for (PinnedChunk &b : buf) {
-    CK(cudaHostAlloc((void **)&b.vals, celems * sizeof(double), cudaHostAllocDefault));
-    CK(cudaHostAlloc((void **)&b.cols, celems * sizeof(int32_t), cudaHostAllocDefault));
-    CK(cudaEventCreateWithFlags(&b.copied, cudaEventDisableTiming));
-  }
+  TRY(p->pinned_staging());
+  bool pending[2] = {false, false};
   bool failed = false;
   std::vector<char> bad(64);
-  for (int64_t c0 = 0, it = 0; c0 < slices && !failed; c0 += kChunkSlices, ++it) {
-    PinnedChunk &b = buf[it & 1];
-    if (b.pending) CK(cudaEventSynchronize(b.copied));
-    b.pending = false;
-    const int64_t c1 = std::min(slices, c0 + kChunkSlices);
+  for (int64_t c0 = 0, it = 0; c0 < slices && !failed; c0 += kPinnedSlices, ++it) {
+    const int h = (int)(it & 1);
+    double *bv = p->pin_vals[h];
+    int32_t *bc = p->pin_cols[h];
+    if (pending[h]) CK(cudaEventSynchronize(p->pin_copied[h]));
+    pending[h] = false;
+    const int64_t c1 = std::min(slices, c0 + kPinnedSlices);
     const int64_t k0 = c0 * HPCGX_SLICE, e0 = c0 * kSliceElems;
     parallel_for((c1 - c0) * HPCGX_SLICE, [&](int64_t a, int64_t e, int t) {
       for (int64_t k = k0 + a; k < k0 + e; ++k) {
-        const int64_t row = natural_row_host(A, k);
+        int ix, iy, iz;
+        const int64_t row = natural_row_host(A, k, ix, iy, iz);
         if (row < 0) {   // padding: value 0, column 0
           for (int s = 0; s < HPCGX_STENCIL; ++s) {
-            b.vals[vidx(k, s) - e0] = 0.0;
-            b.cols[cidx(k, s) - e0] = 0;
+            bv[vidx(k, s) - e0] = 0.0;
+            bc[cidx(k, s) - e0] = 0;
           }
           continue;
         }
-        const std::string m = scan_row(row, [&](int s, int32_t col, double v) {
-          b.vals[vidx(k, s) - e0] = v;
-          b.cols[cidx(k, s) - e0] = col;
-        });
-        if (!m.empty()) {
+        auto put = [&](int s, int32_t col, double v) {
+          bv[vidx(k, s) - e0] = v;
+          bc[cidx(k, s) - e0] = col;
+        };
+        if (!fast_row(row, ix, iy, iz, put) && !scan_row(row, put).empty()) {
           bad[t] = 1;
           return;
         }
@@ -979,15 +1016,13 @@ int load_level_impl(hpcgx_problem *p, int level, Nnz nnz_of, Get get) {
     for (char f : bad) failed |= f != 0;
     if (failed) break;
     const size_t ne = (size_t)(c1 - c0) * kSliceElems;
-    CK(cudaMemcpyAsync(A.vals + e0, b.vals, ne * sizeof(double), cudaMemcpyHostToDevice,
+    CK(cudaMemcpyAsync(A.vals + e0, bv, ne * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+    CK(cudaMemcpyAsync(A.cols + e0, bc, ne * sizeof(int32_t), cudaMemcpyHostToDevice,
                        p->stream));
-    CK(cudaMemcpyAsync(A.cols + e0, b.cols, ne * sizeof(int32_t), cudaMemcpyHostToDevice,
-                       p->stream));
-    CK(cudaEventRecord(b.copied, p->stream));
-    b.pending = true;
+    CK(cudaEventRecord(p->pin_copied[h], p->stream));
+    pending[h] = true;
   }
   CK(cudaStreamSynchronize(p->stream));
-  for (PinnedChunk &b : buf) b.pending = false;
   if (failed) {
     // the lowest failing row: each thread's first in natural order
     std::vector<int64_t> first(64, -1);

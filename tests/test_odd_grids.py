@@ -7,7 +7,8 @@ and empty colours (nx = 1).  Tolerances as in test_gpu_parity.py: SYMGS
 (FP64, and BF16/FP32 with FP64 and FP32 right-hand sides) and the V-cycle
 bit-exact against the oracle's restatement of src/ComputeSYMGS_ref.cpp:67-100
 and src/ComputeMG_ref.cpp:39-63 in colour order; 10 CG iterations to the same
-count with residual norms within 1e-8 relative.
+count with residual norms within 1e-8 relative (or 1e-13 of the initial norm
+once they reach the round-off floor).
 """
 import numpy as np
 import pytest
@@ -79,4 +80,8 @@ def test_vcycles_and_cg(grid, oracle):
     x = torch.zeros(n, dtype=torch.float64, device="cuda")
     k, nr, nr0 = P.cg(cuda(b), x, 10, 0.0)
     ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 10, 0.0, coloured=True)
-    assert k == ok == 10 and abs(nr0 / onr0 - 1) < 1e-14 and abs(nr / onr - 1) < 1e-8
+    # small grids reach the round-off floor within 10 iterations: there the
+    # norms agree to that floor (1e-13 of the initial norm), elsewhere to 1e-8
+    # (1 x 1 x 1 solves exactly in one iteration and stops)
+    assert k == ok and (k == 10 or nr == onr == 0.0) and abs(nr0 / onr0 - 1) < 1e-14
+    assert abs(nr - onr) <= 1e-8 * onr + 1e-13 * onr0
