@@ -417,6 +417,62 @@ def test_load_in_chunks(oracle):
         Q.close()
 
 
+MALFORMED = ["swap", "duplicate", "no_diagonal", "zero", "too_many", "absent_neighbour",
+             "negative"]
+
+
+@pytest.mark.parametrize("kind", MALFORMED)
+def test_load_rejects_malformed_rows(kind, oracle):
+    """The loader's one-pass row check accepts exactly the reference's stencil
+    rows: each malformed row is refused (HPCGX_ELAYOUT) with its own message,
+    the row named, and the level left unloaded until a good load."""
+    from hpcg_b200 import HPCGXError, Problem
+    nx = ny = nz = 16
+    L, _, _, _ = oracle.hierarchy(nx, ny, nz)
+    lev = L[0]
+    nnz, cols, vals = lev.nnz.copy(), lev.cols.reshape(-1, 27).copy(), lev.vals.reshape(-1, 27).copy()
+    row = 5 + nx * (6 + ny * 7)                      # interior: 27 entries, diagonal at 13
+    edge = (nx - 1) + nx * (6 + ny * 7)              # ix = nx - 1: no +x neighbours
+    if kind == "swap":
+        cols[row, [3, 4]] = cols[row, [4, 3]]
+        want = "entries not in stencil order"
+    elif kind == "duplicate":
+        cols[row, 4] = cols[row, 3]
+        want = "entries not in stencil order"
+    elif kind == "no_diagonal":
+        cols[row, 13:26] = cols[row, 14:27].copy()
+        vals[row, 13:26] = vals[row, 14:27].copy()
+        nnz[row] = 26
+        want = "no diagonal"
+    elif kind == "zero":
+        nnz[row] = 0
+        want = "0 entries"
+    elif kind == "too_many":
+        nnz[row] = 28
+        want = "28 entries"
+    elif kind == "absent_neighbour":
+        row = edge
+        k = int(np.argmax(cols[row, :nnz[row]] == row)) + 1   # the entry after the diagonal
+        cols[row, k] = row + 1                        # (0, iy+1): the slot that has no neighbour
+        want = "is not a stencil neighbour"
+    else:
+        cols[row, 0] = -1
+        want = "column out of range"
+    P = Problem(nx, ny, nz, levels=1)
+    try:
+        with pytest.raises(HPCGXError) as e:
+            P.load_level(0, nnz, cols, vals)
+        assert e.value.code == 5 and f"row {row}:" in str(e.value) and want in str(e.value)
+        with pytest.raises(HPCGXError) as e:
+            P.spmv(torch.ones(P.rows(), dtype=torch.float64, device="cuda"), level=0)
+        assert e.value.code == 3
+        P.load_level(0, lev.nnz, lev.cols, lev.vals)
+        u = oracle.uniform(3, lev.nrow)
+        assert (host(P.spmv(cuda(u), level=0)) == oracle.spmv(lev, u)).all()
+    finally:
+        P.close()
+
+
 def test_error_paths(oracle):
     from hpcg_b200 import HPCGXError, Problem
     P = Problem(16, 16, 16)
