@@ -504,11 +504,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    # no legitimate wait between two collectives of this run lasts more than a
+    # few seconds (one problem generation, one solve's per-iteration sums), so
+    # a rank that waits two minutes on its peers has lost one: end with an error
+    os.environ.setdefault("HPCGX_WAIT_TIMEOUT_S", "120")
     if world > 1:
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = local
     torch.cuda.set_device(dev)
 
