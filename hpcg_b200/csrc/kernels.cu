@@ -704,13 +704,15 @@ __device__ __forceinline__ void gs_lines_sym3(const LevelMat<VT> &A, const Class
 template <class VT>
 constexpr int gs_min_blocks() { return std::is_same<VT, uint16_t>::value ? 4 : 2; }
 
+// Lines [jbeg, jend) of the class, lpb per block (a sharded sweep splits its
+// first launch into the lines that read no halo plane and the rest).
 template <int MODE, int DIR, int QS, class VT, class T, class RT>
 __global__ void __launch_bounds__(kThreads, gs_min_blocks<VT>())
-k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, const RT *__restrict__ r, T *x,
-           const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
+k_gs_class(LevelMat<VT> A, ClassInfo C, int lpb, int jbeg, int jend, const RT *__restrict__ r,
+           T *x, const T *__restrict__ xc, T *__restrict__ rc, const int *__restrict__ done) {
   if (done && *done) return;
-  const int j0 = blockIdx.x * lpb;
-  const int j1 = min(j0 + lpb, C.lines);
+  const int j0 = jbeg + blockIdx.x * lpb;
+  const int j1 = min(j0 + lpb, jend);
   gs_lines<MODE, QS, DIR>(A, C, j0, j1, r, x, xc, rc);
 }
 
@@ -1415,11 +1417,11 @@ struct ValsOf<float> {
 // offsets), added to every launch's mode.
 template <int EXTRA, class T, class RT>
 int launch_gs_rows(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                   const T *xc, T *rc, const int *done, cudaStream_t s) {
+                   const T *xc, T *rc, const int *done, cudaStream_t s, int jbeg, int jend) {
   using VT = typename ValsOf<T>::VT;
   const LevelMat<VT> A = mat_of(L, ValsOf<T>::get(L));
-  const dim3 g(L.blocks[q]), b(L.threads[q]);
   const int lpb = L.lines_per_block[q];
+  const dim3 g((unsigned)((jend - jbeg + lpb - 1) / lpb)), b(L.threads[q]);
   const ClassInfo &C = L.cls[q];
   if (mode & GS_SYM3) {
     if (q != 3) return 0;
@@ -1431,38 +1433,40 @@ int launch_gs_rows(const LevelDev &L, int q, int backward, int mode, const RT *r
   }
   if (mode == GS_ZERO_GUESS && !backward) {
     switch (q) {
-      case 0: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
-      case 1: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
-      case 2: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 2><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
-      default: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 3><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done); break;
+      case 0: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done); break;
+      case 1: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 1><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done); break;
+      case 2: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 2><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done); break;
+      default: k_gs_class<GS_ZERO_GUESS | EXTRA, 0, 3><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done); break;
     }
     return 1;
   }
   if (mode == GS_RESTRICT && backward && q == 0) {
-    k_gs_class<GS_RESTRICT | EXTRA, 1, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_RESTRICT | EXTRA, 1, 0><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done);
     return 1;
   }
   if (mode == GS_PROLONG && !backward && q == 0) {
-    k_gs_class<GS_PROLONG | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_PROLONG | EXTRA, 0, 0><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done);
     return 1;
   }
   if (mode != GS_PLAIN) return 0;
   if (backward)
-    k_gs_class<GS_PLAIN | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_PLAIN | EXTRA, 1, -1><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done);
   else
-    k_gs_class<GS_PLAIN | EXTRA, 0, -1><<<g, b, 0, s>>>(A, C, lpb, r, x, xc, rc, done);
+    k_gs_class<GS_PLAIN | EXTRA, 0, -1><<<g, b, 0, s>>>(A, C, lpb, jbeg, jend, r, x, xc, rc, done);
   return 1;
 }
 
 template <class T, class RT>
 int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                    const T *xc, T *rc, const int *done, cudaStream_t s) {
-  if (L.blocks[q] == 0) return 0;
+                    const T *xc, T *rc, const int *done, cudaStream_t s, int jbeg, int jend) {
+  if (jend < 0) jend = L.cls[q].lines;
+  if (L.blocks[q] == 0 || jend <= jbeg) return 0;
+  if ((mode & GS_SYM3) && (jbeg != 0 || jend != L.cls[q].lines)) return 0;   // whole class only
   if constexpr (std::is_same<T, double>::value) {
     if (L.stencil_cols)
-      return launch_gs_rows<GS_STENCIL>(L, q, backward, mode, r, x, xc, rc, done, s);
+      return launch_gs_rows<GS_STENCIL>(L, q, backward, mode, r, x, xc, rc, done, s, jbeg, jend);
   }
-  return launch_gs_rows<0>(L, q, backward, mode, r, x, xc, rc, done, s);
+  return launch_gs_rows<0>(L, q, backward, mode, r, x, xc, rc, done, s, jbeg, jend);
 }
 
 template <class T, class RT>
@@ -1524,13 +1528,13 @@ int launch_rank_sum(int nranks, double *const *bufs, int count, cudaStream_t s) 
 
 template int launch_gs_class<double, double>(const LevelDev &, int, int, int, const double *,
                                              double *, const double *, double *, const int *,
-                                             cudaStream_t);
+                                             cudaStream_t, int, int);
 template int launch_gs_class<float, double>(const LevelDev &, int, int, int, const double *,
                                             float *, const float *, float *, const int *,
-                                            cudaStream_t);
+                                            cudaStream_t, int, int);
 template int launch_gs_class<float, float>(const LevelDev &, int, int, int, const float *,
                                            float *, const float *, float *, const int *,
-                                           cudaStream_t);
+                                           cudaStream_t, int, int);
 
 int launch_waxpby(int64_t n, double alpha, const double *x, double beta, const double *y,
                   double *w, const int *done, cudaStream_t s) {

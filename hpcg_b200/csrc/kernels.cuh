@@ -96,11 +96,13 @@ int launch_get_diagonal(const LevelDev &L, double *diag, cudaStream_t s);
 int launch_spmv(const LevelDev &L, const double *x, double *y, const Reduce *dot, int fin,
                  void *fin_target, const int *done, cudaStream_t s, bool implicit_cols = false);
 int launch_spmv32(const LevelDev &L, const float *x, float *y, cudaStream_t s);
-// One class launch of a Gauss-Seidel half sweep.  T = double (FP64 values and
-// vectors) or float (BF16 values, FP32 vectors); RT is the right-hand side type.
+// One class launch of a Gauss-Seidel half sweep over lines [jbeg, jend) of
+// the class (default: all).  T = double (FP64 values and vectors) or float
+// (BF16 values, FP32 vectors); RT is the right-hand side type.
 template <class T, class RT>
 int launch_gs_class(const LevelDev &L, int q, int backward, int mode, const RT *r, T *x,
-                     const T *xc, T *rc, const int *done, cudaStream_t s);
+                     const T *xc, T *rc, const int *done, cudaStream_t s, int jbeg = 0,
+                     int jend = -1);
 
 
 // Vectors -----------------------------------------------------------------

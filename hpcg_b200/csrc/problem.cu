@@ -103,6 +103,10 @@ struct Step {
   int level = 0;                 // STEP_HALO: level vector vec of esize-byte elements
   void *vec = nullptr;
   int esize = 0;
+  // STEP_HALO: work that reads no halo plane and writes none of the planes
+  // sent, run after the exchange was issued -- beside it where the backend
+  // exchanges on the GPU (NCCL), after it otherwise
+  std::function<int()> interior;
   int fin = -1, nv = 0;          // STEP_SUM: nv totals in gsum, then scalar step fin
 };
 using Plan = std::vector<Step>;
@@ -184,6 +188,17 @@ struct hpcgx_problem {
   double *gsum = nullptr;            // this rank's deferred reduction totals
   double *hstage[kMaxLevels] = {};   // haloed FP64 staging of operator inputs
   bool sharded() const { return nranks > 1 || nccl != nullptr || comm_halo != nullptr; }
+  // side stream and events of the NCCL halo exchanges that run beside
+  // interior work (created on first use)
+  cudaStream_t comm_stream = nullptr;
+  cudaEvent_t ev_ready = nullptr, ev_halo = nullptr;
+  int overlap_streams() {
+    if (comm_stream) return HPCGX_OK;
+    CK(cudaStreamCreateWithFlags(&comm_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ev_halo, cudaEventDisableTiming));
+    return HPCGX_OK;
+  }
   // ---- pinned host staging of the host loaders: two chunks of kPinnedSlices
   // 32-row slices (values and columns), allocated on the first load
   double *pin_vals[2] = {};
@@ -589,12 +604,13 @@ struct hpcgx_problem {
     s.launch = std::move(f);
     pl.push_back(std::move(s));
   }
-  void add_halo(Plan &pl, int l, void *v, int esize) {
+  void add_halo(Plan &pl, int l, void *v, int esize, std::function<int()> interior = {}) {
     Step s;
     s.kind = STEP_HALO;
     s.level = l;
     s.vec = v;
     s.esize = esize;
+    s.interior = std::move(interior);
     pl.push_back(std::move(s));
   }
   void add_sum(Plan &pl, int fin, int nv) {
@@ -614,15 +630,32 @@ struct hpcgx_problem {
     if (A.zhi) CK(cudaMemsetAsync(x + A.n, 0, plane * sizeof(T), stream));
     return HPCGX_OK;
   }
-  // One symmetric sweep of level l (7 class launches) after the halo of x.
-  // xc: the first forward class adds the prolongated correction (GS_PROLONG);
-  // rc: the last backward class forms the restricted residual (GS_RESTRICT).
+  // One symmetric sweep of level l (7 class launches).  xc: the first
+  // forward class adds the prolongated correction (GS_PROLONG); rc: the last
+  // backward class forms the restricted residual (GS_RESTRICT).  halo: the
+  // sweep starts with the halo exchange of x (src/ComputeSYMGS_ref.cpp:56),
+  // and the first launch -- class 0 forward, the planes iz = 0, 2, ... --
+  // runs its lines above plane 0 (which read no halo plane, and write none of
+  // the planes sent) beside the exchange, then the lines of plane 0.  The
+  // halo above is read first by class 2, launches later.
   template <class T, class RT>
   void plan_sweeps(Plan &pl, int l, const RT *r, T *x, bool zero, const int *done,
-                   const T *xc = nullptr, T *rc = nullptr) {
+                   const T *xc = nullptr, T *rc = nullptr, bool halo = false) {
     const int m0 = zero ? GS_ZERO_GUESS : GS_PLAIN;
     for (int q = 0; q < 3; ++q) {
       const int m = (q == 0 && xc) ? GS_PROLONG : m0;
+      if (q == 0 && halo) {
+        const int nyq = L[l].cls[0].nyq;
+        add_halo(pl, l, x, sizeof(T), [=]() {
+          note(launch_gs_class<T, RT>(L[l], 0, 0, m, r, x, xc, nullptr, done, stream, nyq, -1));
+          return HPCGX_OK;
+        });
+        add(pl, [=]() {
+          note(launch_gs_class<T, RT>(L[l], 0, 0, m, r, x, xc, nullptr, done, stream, 0, nyq));
+          return HPCGX_OK;
+        });
+        continue;
+      }
       add(pl, [=]() {
         note(launch_gs_class<T, RT>(L[l], q, 0, m, r, x, xc, nullptr, done, stream));
         return HPCGX_OK;
@@ -698,11 +731,10 @@ struct hpcgx_problem {
         note(launch_prolong<T>(L[l], plane_c, xc, x, done, stream));
         return HPCGX_OK;
       });
-      add_halo(pl, l, x, sizeof(T));
       if (l == 0)
-        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc);
+        plan_sweeps<T, RT0>(pl, 0, r0, x, false, done, xc, nullptr, true);
       else
-        plan_sweeps<T, T>(pl, l, rl(l), x, false, done, xc);
+        plan_sweeps<T, T>(pl, l, rl(l), x, false, done, xc, nullptr, true);
     }
   }
   // The haloed staging vector of level l (operator inputs arrive without halo).
@@ -735,8 +767,8 @@ struct hpcgx_problem {
     double *xs = nullptr;
     TRY(staging_halo(l, &xs));
     plan_copy(pl, x, xs, L[l].n);
-    add_halo(pl, l, xs, sizeof(double));   // src/ComputeSYMGS_ref.cpp:56
-    plan_sweeps<double, double>(pl, l, r, xs, false, nullptr);
+    // the halo exchange of src/ComputeSYMGS_ref.cpp:56 opens the sweep
+    plan_sweeps<double, double>(pl, l, r, xs, false, nullptr, nullptr, nullptr, true);
     plan_copy(pl, xs, x, L[l].n);
     return HPCGX_OK;
   }
@@ -814,8 +846,12 @@ void nccl_release(NcclLink *link);
 
 hpcgx_problem::~hpcgx_problem() {
   cudaSetDevice(device);
+  if (comm_stream) cudaStreamSynchronize(comm_stream);
   if (nccl) nccl_release(nccl);
   if (stream) cudaStreamSynchronize(stream);
+  if (ev_ready) cudaEventDestroy(ev_ready);
+  if (ev_halo) cudaEventDestroy(ev_halo);
+  if (comm_stream) cudaStreamDestroy(comm_stream);
   for (auto &pr : event_pool) {
     cudaEventDestroy(pr.a);
     cudaEventDestroy(pr.b);
@@ -1170,7 +1206,7 @@ namespace {
 // Halo exchange of one level vector of a z-slab over NCCL: this rank's first
 // plane to the rank below (its upper halo), its last plane to the rank above
 // (its lower halo), and the converse into this rank's halo planes.
-int nccl_halo(hpcgx_problem *p, int l, void *v, int esize) {
+int nccl_halo(hpcgx_problem *p, int l, void *v, int esize, cudaStream_t s) {
   const LevelDev &A = p->L[l];
   if (!A.zlo && !A.zhi) return HPCGX_OK;
   NcclApi *api = nccl_api();
@@ -1182,14 +1218,14 @@ int nccl_halo(hpcgx_problem *p, int l, void *v, int esize) {
   // inside a group the calls only record the operations; GroupEnd issues them
   ncclResult_t r = api->GroupStart();
   if (A.zlo && (r == ncclSuccess || r == ncclInProgress)) {
-    r = api->Send(b, plane, t, p->rank - 1, c, p->stream);
+    r = api->Send(b, plane, t, p->rank - 1, c, s);
     if (r == ncclSuccess || r == ncclInProgress)
-      r = api->Recv(b - plane * esize, plane, t, p->rank - 1, c, p->stream);
+      r = api->Recv(b - plane * esize, plane, t, p->rank - 1, c, s);
   }
   if (A.zhi && (r == ncclSuccess || r == ncclInProgress)) {
-    r = api->Send(b + (A.n - (int64_t)plane) * esize, plane, t, p->rank + 1, c, p->stream);
+    r = api->Send(b + (A.n - (int64_t)plane) * esize, plane, t, p->rank + 1, c, s);
     if (r == ncclSuccess || r == ncclInProgress)
-      r = api->Recv(b + A.n * esize, plane, t, p->rank + 1, c, p->stream);
+      r = api->Recv(b + A.n * esize, plane, t, p->rank + 1, c, s);
   }
   const ncclResult_t e = api->GroupEnd();
   if (r == ncclSuccess || r == ncclInProgress) r = e;
@@ -1224,8 +1260,21 @@ int run_plan(hpcgx_problem *p, Plan &pl) {
     if (s.kind == STEP_LAUNCH) {
       TRY(s.launch());
     } else if (s.kind == STEP_HALO) {
-      if (p->nccl) TRY(nccl_halo(p, s.level, s.vec, s.esize));
+      if (p->nccl && s.interior) {
+        // the exchange on the side stream once x is complete; the interior
+        // work beside it; the rest of the plan after it
+        TRY(p->overlap_streams());
+        CK(cudaEventRecord(p->ev_ready, p->stream));
+        CK(cudaStreamWaitEvent(p->comm_stream, p->ev_ready, 0));
+        TRY(nccl_halo(p, s.level, s.vec, s.esize, p->comm_stream));
+        CK(cudaEventRecord(p->ev_halo, p->comm_stream));
+        TRY(s.interior());
+        CK(cudaStreamWaitEvent(p->stream, p->ev_halo, 0));
+        continue;
+      }
+      if (p->nccl) TRY(nccl_halo(p, s.level, s.vec, s.esize, p->stream));
       else if (p->comm_halo) TRY(callback_halo(p, s.level, s.vec, s.esize));
+      if (s.interior) TRY(s.interior());
     } else {
       if (p->nccl)
         NCCLCK(p->nccl, nccl_api()->AllReduce(p->gsum, p->gsum, s.nv, ncclFloat64, ncclSum,
@@ -1287,6 +1336,8 @@ int group_run(hpcgx_group *g, std::vector<Plan> &plans) {
           CK(cudaMemcpyAsync(static_cast<char *>(plans[r - 1][i].vec) + A.n * st.esize, v, pb,
                              cudaMemcpyDeviceToDevice, s));
       }
+      for (int r = 0; r < P; ++r)
+        if (plans[r][i].interior) TRY(plans[r][i].interior());
     } else {
       p0->note(launch_rank_sum(P, g->bufs, s0.nv, s));
       if (s0.fin >= 0)
