@@ -80,3 +80,36 @@ def test_product_fails_loudly_without_library(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(ImportError):
         _lib.lib()
+
+
+def test_header_compiles_and_links_from_c(tmp_path):
+    """include/hpcgx.h is plain C: a C program includes it, links libhpcgx.so
+    and calls through it (a bad geometry is refused with HPCGX_EINVAL before
+    any device is touched; without a GPU, creation fails with a status)."""
+    import shutil
+    import subprocess
+    from hpcg_b200 import _lib
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    src = tmp_path / "use_hpcgx.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "hpcgx.h"
+int main(void) {
+  hpcgx_problem *p = 0;
+  if (hpcgx_version() < 1) return 10;
+  if (hpcgx_create(0, 0, 16, 16, 4, &p) != HPCGX_EINVAL || p) return 11;
+  if (!hpcgx_last_error()[0]) return 12;
+  int rc = hpcgx_create(0, 16, 16, 16, 4, &p);
+  if (rc == HPCGX_OK) { hpcgx_destroy(p); printf("created\n"); return 0; }
+  printf("no device: %d %s\n", rc, hpcgx_last_error());
+  return p == 0 ? 0 : 13;
+}
+''')
+    exe = tmp_path / "use_hpcgx"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L", libdir, "-lhpcgx",
+                    "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
