@@ -194,7 +194,11 @@ struct hpcgx_problem {
   cudaEvent_t ev_ready = nullptr, ev_halo = nullptr;
   int overlap_streams() {
     if (comm_stream) return HPCGX_OK;
-    CK(cudaStreamCreateWithFlags(&comm_stream, cudaStreamNonBlocking));
+    // the highest priority: the exchange's kernels take SM slots as the
+    // interior launch's blocks retire
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&comm_stream, cudaStreamNonBlocking, hi));
     CK(cudaEventCreateWithFlags(&ev_ready, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&ev_halo, cudaEventDisableTiming));
     return HPCGX_OK;
