@@ -245,7 +245,7 @@ struct GeneralProblem {
     spmv(0, p, Ap, done);
     note(launch_dot_finish(n, p, Ap, red, FIN_CG_PAP, st, stream));
     if (capturing) cudaEventRecordWithFlags(phase[precond][3], stream, cudaEventRecordExternal);
-    note(launch_cg_xr(n, p, Ap, x, r, red, st, stream));
+    note(launch_cg_xr(n, p, Ap, x, r, nullptr, red, st, stream));
     if (capturing) cudaEventRecordWithFlags(phase[precond][4], stream, cudaEventRecordExternal);
   }
 };
@@ -482,7 +482,7 @@ int general_cg(GeneralProblem *g, const double *b, double *x, int max_iter, doub
   // p = x, Ap = A p, r = b - Ap, normr0 (src/CG.cpp:86-96)
   GCK(cudaMemcpyAsync(g->p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   g->spmv(0, g->p, g->Ap, nullptr);
-  g->note(launch_cg_init(n, b, g->Ap, g->r, g->red, g->st, s));
+  g->note(launch_cg_init(n, b, g->Ap, g->r, nullptr, g->red, g->st, s));
   // one CUDA graph per iteration, captured on first use for this x
   if (!g->graph[kind] || g->graph_x[kind] != x) {
     if (g->graph[kind]) {

@@ -887,12 +887,13 @@ __global__ void k_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double 
 // r = b - Ap (WAXPBY(1, b, -1, Ap), src/CG.cpp:88) and |r|^2 -> normr0.
 __global__ void __launch_bounds__(kThreads)
 k_cg_init(int64_t n, const double *__restrict__ b, const double *__restrict__ Ap, double *r,
-          Reduce red, CgState *st) {
+          float *r32, Reduce red, CgState *st) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   double acc = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     const double ri = rn_add(b[i], rn_mul(-1.0, Ap[i]));
     r[i] = ri;
+    if (r32) r32[i] = (float)ri;
     acc += ri * ri;
   }
   double v[1] = {acc}, tot[1];
@@ -961,10 +962,11 @@ k_cg_xflush(int64_t n, const double *__restrict__ p, double *x, const CgState *_
 }
 
 // x += alpha p (unless deferred: x null); r -= alpha Ap; |r|^2
-// (src/CG.cpp:121-124).
+// (src/CG.cpp:121-124).  r32 (mixed solver): the FP32 copy of r that the
+// V-cycle's finest level reads -- the value it would round r to itself.
 __global__ void __launch_bounds__(kThreads)
 k_cg_xr(int64_t n, const double *__restrict__ p, const double *__restrict__ Ap, double *x,
-        double *r, Reduce red, CgState *st) {
+        double *r, float *r32, Reduce red, CgState *st) {
   if (st->done) return;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const double alpha = st->alpha, malpha = -st->alpha;
@@ -973,6 +975,7 @@ k_cg_xr(int64_t n, const double *__restrict__ p, const double *__restrict__ Ap, 
     if (x) x[i] = rn_add(x[i], rn_mul(alpha, p[i]));
     const double ri = rn_add(r[i], rn_mul(malpha, Ap[i]));
     r[i] = ri;
+    if (r32) r32[i] = (float)ri;
     acc += ri * ri;
   }
   double v[1] = {acc}, tot[1];
@@ -1588,9 +1591,9 @@ int launch_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double *v, cud
   return 1;
 }
 
-int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, const Reduce &red,
-                   CgState *st, cudaStream_t s) {
-  k_cg_init<<<vector_blocks(n), kThreads, 0, s>>>(n, b, Ap, r, red, st);
+int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, float *r32,
+                   const Reduce &red, CgState *st, cudaStream_t s) {
+  k_cg_init<<<vector_blocks(n), kThreads, 0, s>>>(n, b, Ap, r, r32, red, st);
   return 1;
 }
 
@@ -1623,9 +1626,9 @@ int launch_cg_xflush(int64_t n, const double *p, double *x, const CgState *st, c
   return 1;
 }
 
-int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r,
+int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r, float *r32,
                  const Reduce &red, CgState *st, cudaStream_t s) {
-  k_cg_xr<<<vector_blocks(n), kThreads, 0, s>>>(n, p, Ap, x, r, red, st);
+  k_cg_xr<<<vector_blocks(n), kThreads, 0, s>>>(n, p, Ap, x, r, r32, red, st);
   return 1;
 }
 

@@ -125,8 +125,9 @@ int launch_fill_uniform(int64_t n, uint64_t seed, uint64_t offset, double lo, do
 int launch_fill_normal(int64_t n, uint64_t seed, uint64_t offset, double *v, cudaStream_t s);
 
 // CG pieces ---------------------------------------------------------------
-int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, const Reduce &red,
-                    CgState *st, cudaStream_t s);
+// r32 (may be null): also the FP32 copy of r.
+int launch_cg_init(int64_t n, const double *b, const double *Ap, double *r, float *r32,
+                   const Reduce &red, CgState *st, cudaStream_t s);
 // Index-check record of a -DHPCGX_CHECKED build (0 = clean; else site << 56 |
 // index of the first bad index), cleared by reading; always 0 otherwise.
 // Returns a cudaError_t value.
@@ -154,8 +155,8 @@ template <class ZT>
 int launch_cg_p(int64_t n, const ZT *z, double *p, CgState *st, cudaStream_t s,
                 double *x = nullptr);
 int launch_cg_xflush(int64_t n, const double *p, double *x, const CgState *st, cudaStream_t s);
-int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r,
-                  const Reduce &red, CgState *st, cudaStream_t s);
+int launch_cg_xr(int64_t n, const double *p, const double *Ap, double *x, double *r, float *r32,
+                 const Reduce &red, CgState *st, cudaStream_t s);
 int launch_copy_z(int64_t n, const double *r, double *z, const CgState *st, cudaStream_t s);
 
 // Differentiable solve ----------------------------------------------------

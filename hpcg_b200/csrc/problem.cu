@@ -150,6 +150,11 @@ struct hpcgx_problem {
   // CG work vectors (finest level)
   double *b = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;
   float *z32 = nullptr;
+  // FP32 copy of r, written by the CG update for the mixed V-cycle's finest
+  // level (which reads r on every one of its 14 launches: 4 B a row instead
+  // of 8); HPCGX_R32=0 makes the V-cycle read the FP64 r instead
+  float *r32 = nullptr;
+  bool fine_r32 = env_int("HPCGX_R32", 1) != 0;
   double *tmp = nullptr;      // staging for host diagonals
   double *stage[3] = {};      // staging of the host-buffer operators (allocated on first use)
   double *result = nullptr;   // device scalars of standalone reductions
@@ -244,13 +249,13 @@ struct hpcgx_problem {
   void note(int launched) { launches += launched; }
 
   // ---- byte model of one class launch (for probes)
-  double gs_bytes(int l, int q, int mode, bool mixed) const {
+  double gs_bytes(int l, int q, int mode, bool mixed, double rb0 = 8.0) const {
     const LevelDev &A = L[l];
     // mixed: BF16 value per slot, columns derived from the stencil offsets
     // (FP64 with stencil columns: no column reads either)
     const double vb = mixed ? 2.0 : 8.0, cb = (mixed || A.stencil_cols) ? 0.0 : 4.0;
     const double xb = mixed ? 4.0 : 8.0;
-    const double rb = (mixed && l > 0) ? 4.0 : 8.0;
+    const double rb = l > 0 ? (mixed ? 4.0 : 8.0) : rb0;
     double total = 0.0;
     for (int px = 0; px < 2; ++px) {
       const int c = px + 2 * q, py = q & 1, pz = q >> 1;
@@ -313,7 +318,7 @@ struct hpcgx_problem {
     }
     double bytes = 0.0;
     if ((kinds & probe) || capturing) {
-      bytes = gs_bytes(l, q, sweep, mixed);
+      bytes = gs_bytes(l, q, sweep, mixed, (double)sizeof(RT0));
     }
     return probed(kinds, bytes, [&]() {
       if (l == 0)
@@ -414,6 +419,8 @@ struct hpcgx_problem {
       note(launch_copy_z(n, r, z, st, stream));
     } else if (kind == G_FP64_PREC) {
       TRY((vcycle<double, double>(r, z, done)));
+    } else if (fine_r32) {
+      TRY((vcycle<float, float>(r32, z32, done)));
     } else {
       TRY((vcycle<float, double>(r, z32, done)));
     }
@@ -460,8 +467,9 @@ struct hpcgx_problem {
       return launch_spmv(L[0], p, Ap, &red, FIN_CG_PAP, st, done, stream, implicit_cols);
     }));
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][3], stream, cudaEventRecordExternal));
-    note(launch_cg_xr(n, p, Ap, nullptr, r, red, st, stream));
-    vec_bytes(24.0);
+    float *r32_out = (kind == G_MIXED && fine_r32) ? r32 : nullptr;
+    note(launch_cg_xr(n, p, Ap, nullptr, r, r32_out, red, st, stream));
+    vec_bytes(r32_out ? 28.0 : 24.0);
     if (capturing) CK(cudaEventRecordWithFlags(phase[kind][4], stream, cudaEventRecordExternal));
     return HPCGX_OK;
   }
@@ -541,7 +549,8 @@ struct hpcgx_problem {
     if (xu != x) CK(cudaMemcpyAsync(x, xu, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     CK(cudaMemcpyAsync(p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     note(launch_spmv(L[0], p, Ap, nullptr, 0, nullptr, nullptr, stream, kind == G_MIXED));
-    note(launch_cg_init(n, bu, Ap, r, red, st, stream));
+    note(launch_cg_init(n, bu, Ap, r, (kind == G_MIXED && fine_r32) ? r32 : nullptr, red, st,
+                        stream));
     TRY(build_graph(kind));
     const bool per_iter = tol > 0.0 || probe != HPCGX_PROBE_NONE || times != nullptr;
     double t_mg = 0, t_vec = 0, t_spmv = 0;
@@ -796,7 +805,7 @@ struct hpcgx_problem {
       return HPCGX_OK;
     });
     add(pl, [=]() {
-      note(launch_cg_init(n, bu, Ap, r, deferred(), st, stream));
+      note(launch_cg_init(n, bu, Ap, r, nullptr, deferred(), st, stream));
       return HPCGX_OK;
     });
     add_sum(pl, FIN_CG_INIT, 1);
@@ -839,7 +848,7 @@ struct hpcgx_problem {
     });
     add_sum(pl, FIN_CG_PAP, 1);
     add(pl, [=]() {
-      note(launch_cg_xr(n, p, Ap, nullptr, r, deferred(), st, stream));
+      note(launch_cg_xr(n, p, Ap, nullptr, r, nullptr, deferred(), st, stream));
       return HPCGX_OK;
     });
     add_sum(pl, FIN_CG_RR, 1);
@@ -879,7 +888,8 @@ hpcgx_problem::~hpcgx_problem() {
     if (pin_vals[h]) cudaFreeHost(pin_vals[h]);
     if (pin_cols[h]) cudaFreeHost(pin_cols[h]);
   }
-  for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)Ap, (void *)tmp, (void *)result,
+  for (void *ptr : {(void *)b, (void *)x, (void *)r, (void *)r32, (void *)Ap, (void *)tmp,
+                    (void *)result,
                     (void *)st, (void *)gsum, (void *)red.partials, (void *)red.counter})
     cudaFree(ptr);
   if (gen) general_destroy(gen);
@@ -1547,6 +1557,7 @@ int hpcgx_create_slab(int device, int nx, int ny, int nz, int levels, int nranks
   for (double **v : {&p->z, &p->p})
     if ((rc = p->alloc_halo((void **)v, n, sizeof(double), plane0))) return bail(rc);
   if ((rc = p->alloc_halo((void **)&p->z32, n, sizeof(float), plane0))) return bail(rc);
+  if ((rc = p->alloc((void **)&p->r32, n * sizeof(float)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->gsum, 2 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->result, 4 * sizeof(double)))) return bail(rc);
   if ((rc = p->alloc((void **)&p->st, sizeof(CgState)))) return bail(rc);
