@@ -242,7 +242,10 @@ struct hpcgx_problem {
     void *base = nullptr;
     TRY(alloc(&base, (size_t)(n + 2 * plane) * esize));
     halo_bases.push_back(base);
-    CK(cudaMemset(base, 0, (size_t)(n + 2 * plane) * esize));
+    // zeroed on the problem's stream, ahead of any use there (a plain
+    // cudaMemset runs on the legacy stream, which the problem's non-blocking
+    // stream does not wait for)
+    CK(cudaMemsetAsync(base, 0, (size_t)(n + 2 * plane) * esize, stream));
     *ptr = static_cast<char *>(base) + plane * esize;
     return HPCGX_OK;
   }
@@ -2259,6 +2262,9 @@ int hpcgx_group_create(hpcgx_problem *const *ranks, int nranks, hpcgx_group **ou
   std::vector<double *> h(nranks);
   for (int r = 0; r < nranks; ++r) h[r] = ranks[r]->gsum;
   CK(cudaMemcpy(g->bufs, h.data(), nranks * sizeof(double *), cudaMemcpyHostToDevice));
+  // a pageable copy may still be in flight on the legacy stream, which the
+  // ranks' non-blocking streams do not wait for
+  CK(cudaDeviceSynchronize());
   // one stream for every rank: the lockstep order is the stream order
   for (int r = 0; r < nranks; ++r) {
     CK(cudaStreamSynchronize(ranks[r]->stream));
