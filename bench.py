@@ -733,7 +733,7 @@ def main():
                                          "exceeds the HBM peak; for comparison with other HPCG "
                                          "implementations only"},
         "roofline": roofline(PROBE_SPMV_FINE, "k_spmv<double,double,1,1>"),
-        "roofline_gs_bwd": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f64>"),
+        "roofline_gs_bwd": roofline(PROBE_GS_FINE_BWD, "k_gs_class<0,1,-1,bf16,f32,f32>"),
         "roofline_gs_fine_all_modes": roofline(PROBE_GS_FINE, "k_gs_class finest level, all modes"),
         "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": world * 2 * n * 8,
                 "d2h_bytes_per_step": world * n * 8, "steps": args.steps},
