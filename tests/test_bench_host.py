@@ -26,3 +26,24 @@ def test_flop_model_matches_the_reference_report():
     flops, b64, b32, n0, nnz0 = bench.model((32, 32, 32))
     assert n0 == 32 ** 3 and nnz0 == 830584
     assert 1.0e7 < flops < 1.3e7 and b32 < b64
+
+
+def test_committed_traffic_names_the_kernels_the_bench_reports():
+    """The bench line's `traffic` comes from the small-case ncu capture committed
+    in profiles/roofline_traffic_512.json, looked up by the kernel name the
+    bench reports: every per-kernel roofline of the bench must find its entry,
+    and each entry must say how it was measured."""
+    import json
+    import os
+    import re
+    text = open(os.path.join(ROOT, "bench.py")).read()
+    names = re.findall(r'roofline\(PROBE_\w+, "([^"]+)"\)', text)
+    assert names
+    table = json.load(open(os.path.join(ROOT, "profiles", "roofline_traffic_512.json")))
+    for name in names:
+        if "all modes" in name:
+            continue
+        assert name in table, name
+        entry = table[name]
+        assert entry["dram_bytes_per_launch"] > 0 and entry["passes"] == 1
+        assert "ncu" in entry["command"] and "--clock-control none" in entry["command"]
