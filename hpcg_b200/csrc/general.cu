@@ -3,8 +3,10 @@
 #include "general.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -314,34 +316,47 @@ int general_load_level(GeneralProblem *g, int level, int64_t n, const char *nnz,
   if (coarse && (!f2c || nc < 1 || nc > n))
     return set_error(HPCGX_EINVAL, "every level but the last needs its injection f2c");
   GLevel &A = g->L[level];
-  // ---- checks: entries in range, one diagonal entry per row
+  // ---- checks: entries in range, one diagonal entry per row (on the host's
+  // cores; the failing row with the lowest index is reported)
   std::vector<uint8_t> dposn(n);
-  int64_t bad = -1;
-  std::string badmsg;
-  for (int64_t i = 0; i < n && bad < 0; ++i) {
+  auto check_row = [&](int64_t i, const char **why_row) {
     const int m = (unsigned char)nnz[i];
     if (m < 1) {
-      bad = i;
-      badmsg = "no entries";
-      break;
+      *why_row = "no entries";
+      return false;
     }
     int d = -1;
     for (int j = 0; j < m; ++j) {
       const int32_t c = cols[i][j];
       if (c < 0 || c >= n) {
-        bad = i;
-        badmsg = "column out of range";
-        break;
+        *why_row = "column out of range";
+        return false;
       }
       if (c == i && d < 0) d = j;
     }
-    if (bad < 0 && d < 0) {
-      bad = i;
-      badmsg = "no diagonal entry";
+    if (d < 0) {
+      *why_row = "no diagonal entry";
+      return false;
     }
-    if (bad < 0) dposn[i] = (uint8_t)d;
+    dposn[i] = (uint8_t)d;
+    return true;
+  };
+  std::atomic<int64_t> bad{n};
+  host_parallel(n, [&](int64_t a, int64_t b) {
+    const char *why_row = nullptr;
+    for (int64_t i = a; i < b; ++i)
+      if (!check_row(i, &why_row)) {
+        int64_t seen = bad.load();
+        while (i < seen && !bad.compare_exchange_weak(seen, i)) {
+        }
+        return;
+      }
+  });
+  if (bad.load() < n) {
+    const char *why_row = "";
+    check_row(bad.load(), &why_row);
+    return reject("row " + std::to_string(bad.load()) + ": " + why_row);
   }
-  if (bad >= 0) return reject("row " + std::to_string(bad) + ": " + badmsg);
   if (coarse)
     for (int64_t i = 0; i < nc; ++i)
       if (f2c[i] < 0 || f2c[i] >= n) return reject("f2c entry out of range");
@@ -385,8 +400,12 @@ int general_load_level(GeneralProblem *g, int level, int64_t n, const char *nnz,
     off[s + 1] = off[s] + 32 * (int64_t)w;
   }
   const int64_t entries = off[slices];
-  std::vector<int32_t> hc(entries, 0);
-  std::vector<double> hv(entries, 0.0);
+  // staging written by the host's threads in one pass, padding included
+  // (no serial zero-fill of the 12 B per entry first)
+  std::unique_ptr<int32_t[]> hcp(new int32_t[entries]);
+  std::unique_ptr<double[]> hvp(new double[entries]);
+  int32_t *hc = hcp.get();
+  double *hv = hvp.get();
   std::vector<uint8_t> hn(n), hd(n);
   std::vector<double> hdiag(n);
   host_parallel(n, [&](int64_t a, int64_t b) {
@@ -396,13 +415,26 @@ int general_load_level(GeneralProblem *g, int level, int64_t n, const char *nnz,
       hn[k] = (uint8_t)m;
       hd[k] = dposn[i];
       hdiag[k] = vals[i][dposn[i]];
-      const int64_t base = off[k >> 5] + (k & 31);
+      const int64_t sl = k >> 5, base = off[sl] + (k & 31);
+      const int w = (int)((off[sl + 1] - off[sl]) / 32);
       for (int j = 0; j < m; ++j) {
         hc[base + 32 * j] = cols[i][j];
         hv[base + 32 * j] = vals[i][j];
       }
+      for (int j = m; j < w; ++j) {
+        hc[base + 32 * j] = 0;
+        hv[base + 32 * j] = 0.0;
+      }
     }
   });
+  // lanes of the last slice past the last row
+  for (int64_t k = n; k < 32 * slices; ++k) {
+    const int64_t sl = k >> 5, base = off[sl] + (k & 31);
+    for (int64_t j = 0; j < (off[sl + 1] - off[sl]) / 32; ++j) {
+      hc[base + 32 * j] = 0;
+      hv[base + 32 * j] = 0.0;
+    }
+  }
   // ---- device copies
   A.n = n;
   A.nc = coarse ? nc : 0;
@@ -426,8 +458,8 @@ int general_load_level(GeneralProblem *g, int level, int64_t n, const char *nnz,
   GCK(cudaMemcpyAsync(A.nnz, hn.data(), n, cudaMemcpyHostToDevice, s));
   GCK(cudaMemcpyAsync(A.dpos, hd.data(), n, cudaMemcpyHostToDevice, s));
   GCK(cudaMemcpyAsync(A.perm, perm.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  GCK(cudaMemcpyAsync(A.cols, hc.data(), entries * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  GCK(cudaMemcpyAsync(A.vals, hv.data(), entries * sizeof(double), cudaMemcpyHostToDevice, s));
+  GCK(cudaMemcpyAsync(A.cols, hc, entries * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  GCK(cudaMemcpyAsync(A.vals, hv, entries * sizeof(double), cudaMemcpyHostToDevice, s));
   GCK(cudaMemcpyAsync(A.diag, hdiag.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
   if (coarse) GCK(cudaMemcpyAsync(A.f2c, f2c, nc * sizeof(int32_t), cudaMemcpyHostToDevice, s));
   if (level == 0) {
