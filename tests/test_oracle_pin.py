@@ -127,12 +127,14 @@ def test_testcg_iteration_counts(case, oracle):
         lev.vals[:] = saved
 
 
-def test_live_against_reference_build(oracle):
-    """Fresh seeds against the reference compiled from its sources."""
+@pytest.mark.parametrize("dims", [(24, 16, 32), (40, 24, 56), (64, 32, 16)],
+                         ids=lambda d: "x".join(map(str, d)))
+def test_live_against_reference_build(dims, oracle):
+    """Fresh seeds against the reference compiled from its sources, on the
+    GPU tests' non-cubic grids too (odd coarsest levels: 5 x 3 x 7)."""
     from oracle.oracle import RefProblem
     if not RefProblem.available():
         pytest.skip("oracle/_ref not built (reference sources absent)")
-    dims = (24, 16, 32)
     ref = RefProblem(*dims)
     L, b, _, _ = oracle.hierarchy(*dims)
     oracle.colour_order(L)
