@@ -149,6 +149,17 @@ def test_live_against_reference_build(dims, oracle):
                 ref.symgs_permuted(l, r[:m], x0[:m])).all()
     assert (oracle.mg(L, r) == ref.mg(r)).all()
     assert (oracle.mg(L, r, coloured=True) == ref.mg_permuted(r)).all()
+    # CG_ref's trajectory (src/CG_ref.cpp:58-144), natural and colour order:
+    # same iteration count, norms within 1e-8 after 10 iterations (the
+    # reference's dot products sum in OpenMP's order)
+    b = oracle.spmv(L[0], u)
+    for coloured in (False, True):
+        f = ref.cg_permuted if coloured else ref.cg
+        got = f(b, np.zeros(n), 10, 0.0)
+        ox, ok, onr, onr0 = oracle.cg(L, b, np.zeros(n), 10, 0.0, coloured=coloured)
+        assert got[1] == ok == 10
+        assert abs(got[3] / onr0 - 1) < 1e-13 and abs(got[2] / onr - 1) < 1e-8
+        assert np.abs(got[0] - ox).max() < 1e-10 * np.abs(ox).max()
     ref.close()
 
 
