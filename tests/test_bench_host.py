@@ -47,3 +47,70 @@ def test_committed_traffic_names_the_kernels_the_bench_reports():
         entry = table[name]
         assert entry["dram_bytes_per_launch"] > 0 and entry["passes"] == 1
         assert "ncu" in entry["command"] and "--clock-control none" in entry["command"]
+
+
+def _reference_arm(extra_env=None, *args):
+    import json
+    import os
+    import subprocess
+    env = dict(os.environ)
+    env.update(extra_env or {})
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--ref-sample", "24", "--ref-sample-it", "2"] + list(args),
+                         cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip()]
+    return [json.loads(l) for l in lines]
+
+
+def test_reference_arm_prints_one_contract_line():
+    """`bench.py --impl reference` runs the reference's CG_ref (oracle/_ref) on
+    the host cores, with no GPU, and prints one JSON line on the same metric,
+    unit and direction as the product's arm, its e2e equal to its value with no
+    host-device bytes, and a cpu_baseline that says what was sampled."""
+    import pytest
+    from oracle.oracle import RefProblem, build
+    build()
+    if not RefProblem.available():
+        pytest.skip("oracle/_ref not built (needs the reference sources)")
+    import bench
+    lines = _reference_arm({"RANK": "0"}, "--steps", "2", "--warmup", "1", "--grid", "64")
+    assert len(lines) == 1
+    rec = lines[0]
+    assert rec["impl"] == "reference" and rec["metric"] == bench.METRIC
+    assert rec["unit"] == "s" and rec["higher_is_better"] is False
+    assert rec["steps"] == 2 and rec["warmup"] == 1 and rec["n_gpus"] == 1
+    assert rec["value"] > 0 and abs(rec["ms_per_step"] - rec["value"] * 1e3) < 1e-9 * rec["value"] * 1e3
+    assert rec["e2e"] == {"value": rec["value"], "unit": "s", "h2d_bytes_per_step": 0,
+                          "d2h_bytes_per_step": 0}
+    cb = rec["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["value"] == rec["value"] and cb["cores"] >= 1
+    assert "24^3" in cb["sample"] and cb["sample_grid"] == [24, 24, 24]
+    # 64^3 is a measured iteration count, so nothing about it is extrapolated
+    assert cb["extrapolation"]["iterations"] == bench.REF_NATURAL_ITERS[64]
+    assert cb["extrapolation"]["iterations_basis"] == "measured"
+    assert abs(cb["extrapolation"]["rows_factor"] - (64 / 24) ** 3) < 1e-12
+    assert rec["config"]["grid"] == [64, 64, 64]
+
+
+def test_reference_arm_other_ranks_exit_quietly():
+    """Under torchrun the reference arm runs on rank 0 alone; the other ranks
+    print nothing and exit 0."""
+    assert _reference_arm({"RANK": "1"}, "--steps", "1", "--warmup", "0") == []
+
+
+def test_reference_arm_unavailable_line(monkeypatch, capsys):
+    """Without the reference build the arm prints its one-line `unavailable`
+    record and returns normally."""
+    import argparse
+    import json
+    import bench
+    from oracle import oracle as orc
+    monkeypatch.setattr(orc.RefProblem, "available", classmethod(lambda cls: False))
+    monkeypatch.setenv("RANK", "0")
+    args = argparse.Namespace(gpus=1, steps=1, warmup=0, ref_sample=24, ref_sample_it=1)
+    bench.run_reference(args, (64, 64, 64))
+    out = [l for l in capsys.readouterr().out.splitlines() if l.strip()]
+    assert len(out) == 1
+    rec = json.loads(out[0])
+    assert rec["impl"] == "reference" and "unavailable" in rec
