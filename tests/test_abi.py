@@ -19,6 +19,13 @@ def declared():
     return set(re.findall(r"\b(hpcgx_\w+)\s*\(", text))
 
 
+def status_code(name):
+    """The value of a status macro of include/hpcgx.h."""
+    m = re.search(r"#define\s+%s\s+(\d+)" % name, open(HEADER).read())
+    assert m, name
+    return int(m.group(1))
+
+
 def test_header_declares_the_operator_set():
     names = declared()
     for f in ("hpcgx_cg", "hpcgx_spmv", "hpcgx_symgs", "hpcgx_mg", "hpcgx_dot", "hpcgx_waxpby",
@@ -113,3 +120,32 @@ int main(void) {
                     "-Wl,-rpath," + libdir], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stdout + out.stderr
+
+
+def test_dropin_driver_without_device_reports_every_call(tmp_path):
+    """The reference's driver linked with the drop-in, on a host without a
+    usable CUDA device: OptimizeProblem names the failure, and every replaced
+    operator (CG, SpMV, MG, dot) then returns HPCGX_ESTATE to the driver, which
+    counts the errors (src/main.cpp:190-192); nothing falls back to the
+    reference kernels and no VALID report is written."""
+    import glob
+    import os
+    import subprocess
+    from hpcg_b200.dropin.build import BINARY
+    if not os.path.exists(BINARY):
+        pytest.skip("xhpcg_b200 not built (needs the reference sources at build time)")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="2")
+    out = subprocess.run([BINARY, "--nx=16", "--ny=16", "--nz=16", "--rt=0"], cwd=tmp_path,
+                         env=env, capture_output=True, text=True, timeout=300)
+    # the exit status is the reference driver's own affair (it divides by the
+    # failed CG's zero time later on); the log and the report carry the verdict
+    del out
+    logs = glob.glob(str(tmp_path / "hpcg*T*.txt"))
+    assert len(logs) == 1
+    log = open(logs[0]).read()
+    assert log.splitlines()[0].startswith("OptimizeProblem: hpcgx_create: hpcgx error 2:")
+    state = status_code("HPCGX_ESTATE")
+    for op in ("CG", "SpMV", "MG", "dot"):
+        assert "Error in call to %s: %d." % (op, state) in log, op
+    for report in glob.glob(str(tmp_path / "HPCG-Benchmark_3.1_*.txt")):
+        assert "VALID with a GFLOP/s rating" not in open(report).read()
