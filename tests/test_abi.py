@@ -137,8 +137,8 @@ def test_dropin_driver_without_device_reports_every_call(tmp_path):
     env = dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="2")
     out = subprocess.run([BINARY, "--nx=16", "--ny=16", "--nz=16", "--rt=0"], cwd=tmp_path,
                          env=env, capture_output=True, text=True, timeout=300)
-    # the exit status is the reference driver's own affair (it divides by the
-    # failed CG's zero time later on); the log and the report carry the verdict
+    # the exit status is the reference driver's own affair (src/main.cpp:317
+    # sizes its CG sets by the failed CG's time); the log and report carry the verdict
     del out
     logs = glob.glob(str(tmp_path / "hpcg*T*.txt"))
     assert len(logs) == 1
