@@ -26,6 +26,7 @@ class _Solve(torch.autograd.Function):
     @staticmethod
     def forward(ctx, vals, b, problem, tol, max_iter, mixed):
         problem.set_values(vals.reshape(-1), level=0, recoarsen=True)
+        b = b.contiguous()
         x = torch.zeros_like(b)
         f = problem.cg_mixed if mixed else problem.cg
         k, nr, nr0 = f(b, x, max_iter, tol)

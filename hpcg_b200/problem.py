@@ -33,6 +33,55 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr())
 
 
+F64 = (torch.float64,)
+F32 = (torch.float32,)
+
+
+def _dev(t, n, dtypes, device, name):
+    """The device pointer of a vector argument, after the checks the C ABI
+    cannot make on a raw pointer: a contiguous torch tensor of one of
+    ``dtypes`` on the problem's device with at least ``n`` entries (the
+    kernels read or write that many through the pointer).  A host array or a
+    tensor of another device would be dereferenced by the GPU, and a short or
+    strided one read past its end."""
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name}: expected a torch tensor on {device}, got {type(t).__name__}")
+    if t.device != device:
+        raise ValueError(f"{name}: the tensor is on {t.device}, the problem on {device}")
+    if t.dtype not in dtypes:
+        raise TypeError(f"{name}: dtype {t.dtype}, expected " + " or ".join(map(str, dtypes)))
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: the tensor is not contiguous")
+    if t.numel() < n:
+        raise ValueError(f"{name}: {t.numel()} entries, the operator uses {n}")
+    return C.c_void_p(t.data_ptr())
+
+
+def _host(a, n, name):
+    """The pointer of a host float64 vector (numpy array or CPU tensor, used in
+    place: outputs are written into it) of at least ``n`` entries."""
+    if isinstance(a, torch.Tensor):
+        if a.device.type != "cpu":
+            raise ValueError(f"{name}: expected host memory, the tensor is on {a.device}")
+        a = a.detach().numpy()
+    if not isinstance(a, np.ndarray):
+        raise TypeError(f"{name}: expected a numpy array or CPU tensor, got {type(a).__name__}")
+    if a.dtype != np.float64:
+        raise TypeError(f"{name}: dtype {a.dtype}, expected float64")
+    if not a.flags.c_contiguous:
+        raise ValueError(f"{name}: the array is not contiguous")
+    if a.size < n:
+        raise ValueError(f"{name}: {a.size} entries, the operator uses {n}")
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _at_least(a, n, name):
+    """Size check of a host input array (already converted to its C type)."""
+    if a.size < n:
+        raise ValueError(f"{name}: {a.size} entries, the level needs {n}")
+    return a
+
+
 class Problem:
     """One nx*ny*nz HPCG problem with ``levels`` multigrid levels on a GPU.
 
@@ -80,10 +129,18 @@ class Problem:
         """Rows of any pattern: row i holds nnz[i] entries in cols[i, :nnz[i]] /
         vals[i, :nnz[i]] (2-D arrays, one row per matrix row, entries in the
         order the row sums them); f2c: the injection to the next level."""
-        nnz = np.ascontiguousarray(nnz, np.uint8)
+        nnz = np.ascontiguousarray(nnz, np.uint8).reshape(-1)
         cols = np.ascontiguousarray(cols, np.int32)
         vals = np.ascontiguousarray(vals, np.float64)
+        if cols.ndim != 2 or vals.shape != cols.shape:
+            raise ValueError(f"cols {cols.shape} and vals {vals.shape}: expected two arrays "
+                             "of the same (rows, width) shape")
         n, w = cols.shape
+        if nnz.size != n:
+            raise ValueError(f"nnz: {nnz.size} entries for {n} rows")
+        if n and int(nnz.max()) > w:
+            raise ValueError(f"nnz: a row holds {int(nnz.max())} entries, wider than the "
+                             f"arrays ({w})")
         cptr = (C.c_void_p * n)(*(cols.ctypes.data + 4 * w * np.arange(n)).tolist())
         vptr = (C.c_void_p * n)(*(vals.ctypes.data + 8 * w * np.arange(n)).tolist())
         fc = None if f2c is None else np.ascontiguousarray(f2c, np.int32)
@@ -209,9 +266,10 @@ class Problem:
 
     def load_level(self, level, nnz, cols, vals):
         """Host matrix in the reference's contiguous 27-slot row layout."""
-        nnz = np.ascontiguousarray(nnz, np.uint8)
-        cols = np.ascontiguousarray(cols, np.int32)
-        vals = np.ascontiguousarray(vals, np.float64)
+        n = self.rows(level)
+        nnz = _at_least(np.ascontiguousarray(nnz, np.uint8), n, "nnz")
+        cols = _at_least(np.ascontiguousarray(cols, np.int32), STENCIL * n, "cols")
+        vals = _at_least(np.ascontiguousarray(vals, np.float64), STENCIL * n, "vals")
         check(lib().hpcgx_load_level(self.h, level, _ptr(nnz), _ptr(cols), _ptr(vals)))
         self.values_version += 1
 
@@ -228,7 +286,7 @@ class Problem:
         check(lib().hpcgx_set_stencil_columns(self.h, int(bool(on))))
 
     def set_diagonal(self, level, diag):
-        d = np.ascontiguousarray(diag, np.float64)
+        d = _at_least(np.ascontiguousarray(diag, np.float64), self.rows(level), "diag")
         check(lib().hpcgx_set_diagonal_host(self.h, level, _ptr(d)))
         self.values_version += 1
 
@@ -240,7 +298,9 @@ class Problem:
     def set_values(self, vals27, level=0, recoarsen=False):
         self._pre()
         v = vals27.contiguous()
-        check(lib().hpcgx_set_values(self.h, level, _ptr(v), int(recoarsen)))
+        check(lib().hpcgx_set_values(self.h, level,
+                                     _dev(v, STENCIL * self.rows(level), F64, self.device,
+                                          "vals27"), int(recoarsen)))
         self.values_version += 1
 
     def get_values(self, level=0):
@@ -257,102 +317,124 @@ class Problem:
         return b.value
 
     # ----------------------------------------------------------- operators
+    def _v(self, t, level, name, dtypes=F64):
+        return _dev(t, self.rows(level), dtypes, self.device, name)
+
     def spmv(self, x, level=0, y=None, stencil_cols=False):
         """y = A x; stencil_cols derives the columns from the stencil offsets."""
         self._pre()
         y = self.empty(level) if y is None else y
         f = lib().hpcgx_spmv_stencil if stencil_cols else lib().hpcgx_spmv
-        check(f(self.h, level, _ptr(x), _ptr(y)))
+        check(f(self.h, level, self._v(x, level, "x"), self._v(y, level, "y")))
         return y
 
     def symgs(self, r, x, level=0):
         """One symmetric Gauss-Seidel sweep, x updated in place."""
         self._pre()
-        check(lib().hpcgx_symgs(self.h, level, _ptr(r), _ptr(x)))
+        check(lib().hpcgx_symgs(self.h, level, self._v(r, level, "r"), self._v(x, level, "x")))
         return x
 
     def mg(self, r, x=None):
         self._pre()
         x = self.empty(0) if x is None else x
-        check(lib().hpcgx_mg(self.h, _ptr(r), _ptr(x)))
+        check(lib().hpcgx_mg(self.h, self._v(r, 0, "r"), self._v(x, 0, "x")))
         return x
 
     def restriction(self, level, rf, Axf):
         self._pre()
         rc = self.empty(level + 1)
-        check(lib().hpcgx_restriction(self.h, level, _ptr(rf), _ptr(Axf), _ptr(rc)))
+        check(lib().hpcgx_restriction(self.h, level, self._v(rf, level, "rf"),
+                                      self._v(Axf, level, "Axf"), _ptr(rc)))
         return rc
 
     def prolongation(self, level, xc, xf):
         self._pre()
-        check(lib().hpcgx_prolongation(self.h, level, _ptr(xc), _ptr(xf)))
+        check(lib().hpcgx_prolongation(self.h, level, self._v(xc, level + 1, "xc"),
+                                       self._v(xf, level, "xf")))
         return xf
+
+    def _n(self, x, name="x"):
+        """n of a length-n vector operation: all of x, on the problem's device."""
+        return _dev(x, 0, F64, self.device, name), x.numel()
 
     def dot(self, x, y):
         self._pre()
+        px, n = self._n(x)
         out = C.c_double()
-        check(lib().hpcgx_dot(self.h, x.numel(), _ptr(x), _ptr(y), C.byref(out)))
+        check(lib().hpcgx_dot(self.h, n, px, _dev(y, n, F64, self.device, "y"), C.byref(out)))
         return out.value
 
     def waxpby(self, alpha, x, beta, y, w=None):
         self._pre()
+        px, n = self._n(x)
         w = torch.empty_like(x) if w is None else w
-        check(lib().hpcgx_waxpby(self.h, x.numel(), float(alpha), _ptr(x), float(beta), _ptr(y),
-                                 _ptr(w)))
+        check(lib().hpcgx_waxpby(self.h, n, float(alpha), px, float(beta),
+                                 _dev(y, n, F64, self.device, "y"),
+                                 _dev(w, n, F64, self.device, "w")))
         return w
 
     def residual(self, v1, v2):
         self._pre()
+        p1, n = self._n(v1, "v1")
         out = C.c_double()
-        check(lib().hpcgx_residual(self.h, v1.numel(), _ptr(v1), _ptr(v2), C.byref(out)))
+        check(lib().hpcgx_residual(self.h, n, p1, _dev(v2, n, F64, self.device, "v2"),
+                                   C.byref(out)))
         return out.value
 
     # mixed precision --------------------------------------------------
     def spmv_mixed(self, x32, level=0):
         self._pre()
         y = self.empty(level, torch.float32)
-        check(lib().hpcgx_spmv_mixed(self.h, level, _ptr(x32), _ptr(y)))
+        check(lib().hpcgx_spmv_mixed(self.h, level, self._v(x32, level, "x32", F32), _ptr(y)))
         return y
 
     def symgs_mixed(self, r, x32, level=0):
+        """One FP32 sweep with BF16 values; r is float64 or float32."""
         self._pre()
-        r64 = r if r.dtype == torch.float64 else None
-        r32 = r if r.dtype == torch.float32 else None
-        check(lib().hpcgx_symgs_mixed(self.h, level, _ptr(r64), _ptr(r32), _ptr(x32)))
+        pr = self._v(r, level, "r", F64 + F32)
+        r64, r32 = (pr, None) if r.dtype == torch.float64 else (None, pr)
+        check(lib().hpcgx_symgs_mixed(self.h, level, r64, r32, self._v(x32, level, "x32", F32)))
         return x32
 
     def mg_mixed(self, r, x32=None):
         self._pre()
         x32 = self.empty(0, torch.float32) if x32 is None else x32
-        check(lib().hpcgx_mg_mixed(self.h, _ptr(r), _ptr(x32)))
+        check(lib().hpcgx_mg_mixed(self.h, self._v(r, 0, "r"), self._v(x32, 0, "x32", F32)))
         return x32
 
     # ----------------------------------------------------------- solvers
+    def _times(self, times):
+        """CG's host times array: the library adds to entries 0 (total), 2
+        (vector operations), 3 (SpMV) and 5 (preconditioner), the slots of
+        src/CG.cpp:133-141."""
+        return None if times is None else _host(times, 6, "times")
+
     def cg(self, b, x, max_iter, tol, precond=True, times=None):
         """Returns (niters, normr, normr0); x is updated in place."""
         self._pre()
         it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
-        tp = _ptr(times) if times is not None else None
-        check(lib().hpcgx_cg(self.h, _ptr(b), _ptr(x), int(max_iter), float(tol), int(precond),
-                             C.byref(it), C.byref(nr), C.byref(nr0), tp))
+        check(lib().hpcgx_cg(self.h, self._v(b, 0, "b"), self._v(x, 0, "x"), int(max_iter),
+                             float(tol), int(precond), C.byref(it), C.byref(nr), C.byref(nr0),
+                             self._times(times)))
         return it.value, nr.value, nr0.value
 
     def cg_mixed(self, b, x, max_iter, tol, times=None):
         self._pre()
         it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
-        tp = _ptr(times) if times is not None else None
-        check(lib().hpcgx_cg_mixed(self.h, _ptr(b), _ptr(x), int(max_iter), float(tol),
-                                   C.byref(it), C.byref(nr), C.byref(nr0), tp))
+        check(lib().hpcgx_cg_mixed(self.h, self._v(b, 0, "b"), self._v(x, 0, "x"),
+                                   int(max_iter), float(tol), C.byref(it), C.byref(nr),
+                                   C.byref(nr0), self._times(times)))
         return it.value, nr.value, nr0.value
 
     def cg_host(self, b_host, x_host, max_iter, tol, mixed=False, precond=True, times=None):
         """Solve from host buffers (numpy or pinned CPU tensors); x_host updated."""
         self._pre()
         it, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
-        tp = _ptr(times) if times is not None else None
+        n = self.rows(0)
         mode = _lib.CG_MIXED if mixed else (_lib.CG_MG if precond else _lib.CG_PLAIN)
-        check(lib().hpcgx_cg_host(self.h, mode, _ptr(b_host), _ptr(x_host), int(max_iter),
-                                  float(tol), C.byref(it), C.byref(nr), C.byref(nr0), tp))
+        check(lib().hpcgx_cg_host(self.h, mode, _host(b_host, n, "b_host"),
+                                  _host(x_host, n, "x_host"), int(max_iter), float(tol),
+                                  C.byref(it), C.byref(nr), C.byref(nr0), self._times(times)))
         return it.value, nr.value, nr0.value
 
     # ----------------------------------------------------------- adjoint
@@ -360,7 +442,8 @@ class Problem:
         self._pre()
         n = self.rows(0)
         g = torch.empty(n * STENCIL, dtype=torch.float64, device=self.device)
-        check(lib().hpcgx_adjoint_grad(self.h, _ptr(lam), _ptr(x), _ptr(g)))
+        check(lib().hpcgx_adjoint_grad(self.h, self._v(lam, 0, "lam"), self._v(x, 0, "x"),
+                                       _ptr(g)))
         return g.view(n, STENCIL)
 
     # ----------------------------------------------------------- inputs
@@ -426,8 +509,6 @@ class _DeviceArray:
                                          "data": (ptr, False), "version": 3, "strides": None}
 
 
-def _ptrs(ts):
-    return (C.c_void_p * len(ts))(*[t.data_ptr() for t in ts])
 
 
 class Group:
@@ -462,28 +543,39 @@ class Group:
     def _pre(self):
         self.stream.wait_stream(torch.cuda.current_stream(self.ranks[0].device))
 
+    def _ptrs(self, ts, level, name):
+        """One checked device pointer per rank (see _dev)."""
+        if len(ts) != len(self.ranks):
+            raise ValueError(f"{name}: {len(ts)} vectors for {len(self.ranks)} ranks")
+        return (C.c_void_p * len(ts))(*[
+            _dev(t, p.rows(level), F64, p.device, "%s[%d]" % (name, i)).value
+            for i, (t, p) in enumerate(zip(ts, self.ranks))])
+
     def spmv(self, xs, level=0):
         self._pre()
         ys = [p.empty(level) for p in self.ranks]
-        check(lib().hpcgx_group_spmv(self.g, level, _ptrs(xs), _ptrs(ys)))
+        check(lib().hpcgx_group_spmv(self.g, level, self._ptrs(xs, level, "xs"),
+                                     self._ptrs(ys, level, "ys")))
         return ys
 
     def symgs(self, rs, xs, level=0):
         """One symmetric sweep per slab (block Jacobi across slabs), x in place."""
         self._pre()
-        check(lib().hpcgx_group_symgs(self.g, level, _ptrs(rs), _ptrs(xs)))
+        check(lib().hpcgx_group_symgs(self.g, level, self._ptrs(rs, level, "rs"),
+                                      self._ptrs(xs, level, "xs")))
         return xs
 
     def mg(self, rs):
         self._pre()
         xs = [p.empty(0) for p in self.ranks]
-        check(lib().hpcgx_group_mg(self.g, _ptrs(rs), _ptrs(xs)))
+        check(lib().hpcgx_group_mg(self.g, self._ptrs(rs, 0, "rs"), self._ptrs(xs, 0, "xs")))
         return xs
 
     def cg(self, bs, xs, max_iter, tol, mode=_lib.CG_MG):
         """CG over the slabs; xs updated in place; returns (iters, normr, normr0)."""
         self._pre()
         k, nr, nr0 = C.c_int(), C.c_double(), C.c_double()
-        check(lib().hpcgx_group_cg(self.g, mode, _ptrs(bs), _ptrs(xs), max_iter, tol,
+        check(lib().hpcgx_group_cg(self.g, mode, self._ptrs(bs, 0, "bs"), self._ptrs(xs, 0, "xs"),
+                                   max_iter, tol,
                                    C.byref(k), C.byref(nr), C.byref(nr0)))
         return k.value, nr.value, nr0.value
