@@ -32,6 +32,7 @@ SUM_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
 SIGNATURES = {
     "hpcgx_last_error": (C.c_char_p, []),
     "hpcgx_version": (_I, []),
+    "hpcgx_init_device": (_I, [_I]),
     "hpcgx_create": (_I, [_I, _I, _I, _I, _I, C.POINTER(_P)]),
     "hpcgx_destroy": (_I, [_P]),
     "hpcgx_load_level": (_I, [_P, _I, _P, _P, _P]),

@@ -1497,6 +1497,13 @@ const char *hpcgx_last_error(void) { return g_err.c_str(); }
 
 int hpcgx_version(void) { return 2; }   // 2: sharding (slabs, NCCL, groups)
 
+int hpcgx_init_device(int device) {
+  NvtxRange range_("hpcgx_init_device");
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaFree(nullptr);   // forces the context into existence
+  return e == cudaSuccess ? HPCGX_OK : cuda_fail(e);
+}
+
 int hpcgx_create(int device, int nx, int ny, int nz, int levels, hpcgx_problem **out) {
   return hpcgx_create_slab(device, nx, ny, nz, levels, 1, 0, out);
 }

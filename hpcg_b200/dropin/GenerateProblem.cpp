@@ -20,8 +20,11 @@
 #include <cassert>
 
 #include "GenerateProblem.hpp"
+#include "hpcgx_dropin.hpp"
 
 void GenerateProblem(SparseMatrix &A, Vector *b, Vector *x, Vector *xexact) {
+  // the CUDA context is made on another thread while the host builds the rows
+  hpcgx_dropin::start_device_init();
   const global_int_t nx = A.geom->nx, ny = A.geom->ny, nz = A.geom->nz;
   const global_int_t gnx = A.geom->gnx, gny = A.geom->gny, gnz = A.geom->gnz;
   const global_int_t gix0 = A.geom->gix0, giy0 = A.geom->giy0, giz0 = A.geom->giz0;

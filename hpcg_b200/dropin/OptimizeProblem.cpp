@@ -43,8 +43,8 @@ int OptimizeProblem(SparseMatrix &A, CGData &data, Vector &b, Vector &x, Vector 
   }
   int levels = 1;
   for (const SparseMatrix *m = &A; m->mgData; m = m->Ac) ++levels;
-  const char *dev = std::getenv("HPCGX_DEVICE");
-  const int device = dev ? std::atoi(dev) : 0;
+  const int device = hpcgx_dropin::device();
+  hpcgx_dropin::wait_device_init();
   const char *gen = std::getenv("HPCGX_DROPIN_GENERAL");
   hpcgx_problem *p = nullptr;
   int rc = HPCGX_ELAYOUT;

@@ -44,7 +44,7 @@ def build(force: bool = False) -> str | None:
     # line 101) that allocates each level's rows as one block instead of one
     # allocation per row; it shortens set-up and is honoured alike by
     # GenerateProblem.cpp here and the reference's DeleteMatrix.
-    cmd = ["g++", "-O3", "-fno-fast-math", "-ffp-contract=off", "-fopenmp", "-DHPCG_NO_MPI",
+    cmd = ["g++", "-O3", "-fno-fast-math", "-ffp-contract=off", "-fopenmp", "-pthread", "-DHPCG_NO_MPI",
            "-DHPCG_CONTIGUOUS_ARRAYS", "-w",
            "-I", REF, "-I", HERE, "-I", os.path.join(ROOT, "include"), "-o", BINARY,
            *ref_srcs, *ours, lib, "-Wl,-rpath,$ORIGIN/../.."]

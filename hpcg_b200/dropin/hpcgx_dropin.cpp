@@ -1,7 +1,9 @@
 // hpcgx_dropin.cpp -- helpers of the drop-in operator files.
 #include "hpcgx_dropin.hpp"
 
+#include <cstdlib>
 #include <fstream>
+#include <thread>
 
 #include "hpcg.hpp"
 
@@ -9,6 +11,31 @@ namespace hpcgx_dropin {
 
 namespace {
 hpcgx_problem *g_current = nullptr;
+
+// Joined by wait_device_init, or at exit if the driver never optimizes.
+struct DeviceInit {
+  std::thread t;
+  bool started = false;
+  ~DeviceInit() {
+    if (t.joinable()) t.join();
+  }
+} g_init;
+}  // namespace
+
+int device() {
+  const char *dev = std::getenv("HPCGX_DEVICE");
+  return dev ? std::atoi(dev) : 0;
+}
+
+void start_device_init() {
+  if (g_init.started) return;
+  g_init.started = true;
+  const int d = device();
+  g_init.t = std::thread([d] { (void)hpcgx_init_device(d); });
+}
+
+void wait_device_init() {
+  if (g_init.t.joinable()) g_init.t.join();
 }
 
 hpcgx_problem *current() { return g_current; }

@@ -40,6 +40,18 @@ int sync_diagonals(const SparseMatrix &A);
 // Returns rc; on failure also logs the library's message to HPCG_fout.
 int report(int rc, const char *where);
 
+// The GPU the drop-in runs on: HPCGX_DEVICE, else 0.
+int device();
+
+// Creating the CUDA context is the process's first CUDA call and takes about
+// a second.  GenerateProblem starts it on a thread of its own
+// (hpcgx_init_device), where it overlaps the host's problem generation, and
+// OptimizeProblem waits for that thread before its first library call.  The
+// thread's status is not reported: if the context cannot be made,
+// OptimizeProblem's own hpcgx_create fails and says why.
+void start_device_init();
+void wait_device_init();
+
 }  // namespace hpcgx_dropin
 
 #endif

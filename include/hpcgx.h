@@ -45,6 +45,12 @@ typedef struct hpcgx_group hpcgx_group;
 
 const char *hpcgx_last_error(void);
 int hpcgx_version(void);
+/* Makes `device` the calling thread's device and creates its CUDA context
+ * (the process's first CUDA call, about a second), so that a later
+ * hpcgx_create finds it ready.  Any thread may call it: the context is
+ * shared by the process.  No counterpart in the reference; the drop-in
+ * starts it on a thread of its own while the host builds the problem. */
+int hpcgx_init_device(int device);
 
 /* ---- problem set-up: OptimizeProblem (src/OptimizeProblem.hpp:22) ------ */
 

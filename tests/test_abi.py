@@ -69,6 +69,7 @@ def test_create_without_gpu_returns_status():
     rc = _lib.lib().hpcgx_create(0, 16, 16, 16, 4, C.byref(h))
     assert rc == 2 and not h.value
     assert _lib.lib().hpcgx_last_error()
+    assert _lib.lib().hpcgx_init_device(0) == 2
 
 
 def test_bad_arguments_rejected_before_any_device_work():
