@@ -1,4 +1,5 @@
-"""The sharded (z-slab) algorithm on CPU ranks (gloo, world size 2).
+"""The sharded (z-slab) algorithm on CPU ranks (gloo, world sizes 2 and 3:
+edge ranks with one neighbour, and an interior rank with two).
 
 Each rank does what the reference's MPI build does on a 1 x 1 x 2 process
 grid: it holds only its own slab (rows with local numbering, columns of the
@@ -20,6 +21,7 @@ import os
 import socket
 
 import numpy as np
+import pytest
 import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
@@ -27,7 +29,6 @@ import torch.multiprocessing as mp
 from conftest import ROOT
 
 LOCAL = (16, 8, 8)      # nx, ny, nz per rank
-RANKS = 2
 
 
 def _free_port():
@@ -176,9 +177,18 @@ def _worker(rank, world, port, out):
                      _p(s.order), _p(r), _p(e, s.plane))
 
     def dot(x, y):
+        """The ranks' partial dots added in rank order, as the oracle's
+        restatement and the library's in-process group add them.  An
+        all-reduce (MPI_Allreduce in src/ComputeDotProduct_ref.cpp:66-77,
+        gloo's, NCCL's) fixes no order of the additions, which from three
+        ranks on can change the last bits of the total."""
         local = torch.tensor([lib.or_dot(C.c_int64(x.size), _p(x), _p(y))], dtype=torch.float64)
-        dist.all_reduce(local)
-        return float(local[0])
+        parts = [torch.zeros(1, dtype=torch.float64) for _ in range(world)]
+        dist.all_gather(parts, local)
+        total = 0.0
+        for t in parts:
+            total += float(t[0])
+        return total
 
     def waxpby(a, x, b, y):
         w = np.zeros_like(x)
@@ -243,20 +253,21 @@ def _worker(rank, world, port, out):
     dist.destroy_process_group()
 
 
-def test_slab_oracle_matches_per_rank_exchange_two_gloo_ranks(oracle):
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_oracle_matches_per_rank_exchange_gloo_ranks(world, oracle):
     port = _free_port()
     mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
-    mp.start_processes(_worker, args=(RANKS, port, out), nprocs=RANKS, join=True,
+    mp.start_processes(_worker, args=(world, port, out), nprocs=world, join=True,
                        start_method="spawn")
     nx, ny, nz = LOCAL
-    L, _, _, _ = oracle.slab_hierarchy(nx, ny, nz, RANKS)
+    L, _, _, _ = oracle.slab_hierarchy(nx, ny, nz, world)
     oracle.colour_order(L)
     n = L[0].nrow
     u = oracle.uniform(11, n, 1.0, 2.0)
     rr = oracle.uniform(12, n)
     x0 = oracle.uniform(13, n)
-    cat = lambda key: np.concatenate([out[r][key] for r in range(RANKS)])  # noqa: E731
+    cat = lambda key: np.concatenate([out[r][key] for r in range(world)])  # noqa: E731
     assert (cat("spmv") == oracle.spmv(L[0], u)).all()
     assert (cat("symgs") == oracle.symgs(L[0], rr, x0, coloured=True)).all()
     assert (cat("mg") == oracle.mg(L, rr, coloured=True)).all()
