@@ -386,6 +386,8 @@ class RefProblem:
             lib = C.CDLL(LIBREF)
             lib.ref_create.restype = _P
             lib.ref_create.argtypes = [C.c_int, C.c_int, C.c_int]
+            lib.ref_create_levels.restype = _P
+            lib.ref_create_levels.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
             lib.ref_destroy.argtypes = [_P]
             lib.ref_level_rows.restype = _I64
             lib.ref_level_rows.argtypes = [_P, C.c_int]
@@ -415,9 +417,15 @@ class RefProblem:
             cls._lib = lib
         return cls._lib
 
-    def __init__(self, nx, ny, nz):
-        self.h = self.lib().ref_create(nx, ny, nz)
-        self.dims = [(nx >> l, ny >> l, nz >> l) for l in range(LEVELS)]
+    def __init__(self, nx, ny, nz, levels=LEVELS):
+        """The reference's set-up (src/main.cpp:116-159) with ``levels``
+        levels; every level but the last needs even dimensions."""
+        self.h = None
+        self.levels = levels
+        self.h = self.lib().ref_create_levels(nx, ny, nz, levels)
+        if not self.h:
+            raise ValueError("levels must be 1..%d" % LEVELS)
+        self.dims = [(nx >> l, ny >> l, nz >> l) for l in range(levels)]
 
     def close(self):
         if self.h:
@@ -439,7 +447,7 @@ class RefProblem:
         cols = np.zeros(n * STENCIL, np.int32)
         vals = np.zeros(n * STENCIL)
         diag = np.zeros(n, np.int32)
-        f2c = np.zeros(n // 8, np.int32) if level + 1 < LEVELS else None
+        f2c = np.zeros(self.rows(level + 1), np.int32) if level + 1 < self.levels else None
         self.lib().ref_export_level(self.h, level, _ptr(nnz), _ptr(cols), _ptr(vals), _ptr(diag),
                                     _ptr(f2c))
         nx, ny, nz = self.dims[level]

@@ -43,6 +43,7 @@ namespace {
 const int kLevels = 4;  // src/main.cpp:139
 
 struct RefProblem {
+  int nlev = kLevels;     // levels built (fewer for grids that do not coarsen 3 times)
   Geometry *geom = nullptr;
   SparseMatrix A;
   Vector b, x, xexact;
@@ -123,20 +124,24 @@ void free_permuted(SparseMatrix *P) {
 
 extern "C" {
 
-void *ref_create(int nx, int ny, int nz) {
+// The reference's set-up with `levels` multigrid levels (1..4): every level but
+// the last must have even dimensions (GenerateCoarseProblem asserts it).
+void *ref_create_levels(int nx, int ny, int nz, int levels) {
+  if (levels < 1 || levels > kLevels) return nullptr;
   RefProblem *p = new RefProblem;
+  p->nlev = levels;
   p->geom = new Geometry;
   GenerateGeometry(1, 0, 1, 0, 0, 0, nx, ny, nz, 1, 1, 1, p->geom);
   InitializeSparseMatrix(p->A, p->geom);
   GenerateProblem(p->A, &p->b, &p->x, &p->xexact);
   SetupHalo(p->A);
   SparseMatrix *cur = &p->A;
-  for (int l = 1; l < kLevels; ++l) {
+  for (int l = 1; l < p->nlev; ++l) {
     GenerateCoarseProblem(*cur);
     cur = cur->Ac;
   }
   cur = &p->A;
-  for (int l = 0; l < kLevels; ++l) {
+  for (int l = 0; l < p->nlev; ++l) {
     p->level[l] = cur;
     CheckProblem(*cur, l == 0 ? &p->b : nullptr, l == 0 ? &p->x : nullptr,
                  l == 0 ? &p->xexact : nullptr);
@@ -145,6 +150,8 @@ void *ref_create(int nx, int ny, int nz) {
   InitializeSparseCGData(p->A, p->data);
   return p;
 }
+
+void *ref_create(int nx, int ny, int nz) { return ref_create_levels(nx, ny, nz, kLevels); }
 
 void ref_destroy(void *h) {
   RefProblem *p = static_cast<RefProblem *>(h);
@@ -285,14 +292,14 @@ int ref_cg(void *h, const double *b, double *x, int max_iter, double tol, int pr
 int ref_build_permuted(void *h, const int64_t *const *positions) {
   RefProblem *p = static_cast<RefProblem *>(h);
   if (!p->perm.empty()) return 0;
-  p->pos.resize(kLevels);
-  for (int l = 0; l < kLevels; l++) {
+  p->pos.resize(p->nlev);
+  for (int l = 0; l < p->nlev; l++) {
     local_int_t n = p->level[l]->localNumberOfRows;
     p->pos[l].resize(n);
     for (local_int_t i = 0; i < n; i++) p->pos[l][i] = (local_int_t)positions[l][i];
     p->perm.push_back(permuted_copy(*p->level[l], p->pos[l]));
   }
-  for (int l = 0; l + 1 < kLevels; l++) {
+  for (int l = 0; l + 1 < p->nlev; l++) {
     const SparseMatrix &A = *p->level[l];
     local_int_t nc = A.mgData->rc->localLength;
     local_int_t *f2c = new local_int_t[A.localNumberOfRows];

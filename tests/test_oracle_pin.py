@@ -163,6 +163,56 @@ def test_live_against_reference_build(dims, oracle):
     ref.close()
 
 
+ODD_GRIDS = [(15, 13, 11, 1), (9, 7, 5, 1), (1, 6, 3, 1), (3, 1, 2, 1), (1, 1, 1, 1),
+             (65, 13, 11, 1), (30, 26, 22, 2), (40, 24, 56, 3), (128, 40, 24, 2)]
+
+
+@pytest.mark.parametrize("grid", ODD_GRIDS, ids=lambda d: "x".join(map(str, d[:3])) + f"_l{d[3]}")
+def test_live_reference_on_odd_and_shallow_grids(grid, oracle):
+    """The grids of the GPU's odd-grid tests, against the reference built
+    with as many levels as the grid coarsens (odd, degenerate and single-row
+    grids; 1 to 3 levels): the generated matrix and injection, SpMV, SYMGS in
+    natural and colour order, the V-cycle and CG_ref's trajectory."""
+    from oracle.oracle import RefProblem
+    if not RefProblem.available():
+        pytest.skip("oracle/_ref not built (reference sources absent)")
+    nx, ny, nz, levels = grid
+    ref = RefProblem(nx, ny, nz, levels=levels)
+    try:
+        L, b, _, _ = oracle.hierarchy(nx, ny, nz, levels=levels)
+        oracle.colour_order(L)
+        ref.build_permuted([lev.position for lev in L])
+        for l, lev in enumerate(L):
+            got = ref.export_level(l)
+            assert (got.nnz == lev.nnz).all() and (got.cols == lev.cols).all()
+            assert (got.vals == lev.vals).all() and (got.diag == lev.diag).all()
+            assert (got.f2c is None) == (lev.f2c is None)
+            if lev.f2c is not None:
+                assert (got.f2c == lev.f2c).all()
+        n = L[0].nrow
+        u, r, x0 = oracle.uniform(111, n, -1, 1), oracle.uniform(112, n), oracle.uniform(113, n)
+        for l, lev in enumerate(L):
+            m = lev.nrow
+            assert (oracle.spmv(lev, u[:m]) == ref.spmv(l, u[:m])).all()
+            assert (oracle.symgs(lev, r[:m], x0[:m]) == ref.symgs(l, r[:m], x0[:m])).all()
+            assert (oracle.symgs(lev, r[:m], x0[:m], coloured=True) ==
+                    ref.symgs_permuted(l, r[:m], x0[:m])).all()
+        assert (oracle.mg(L, r) == ref.mg(r)).all()
+        assert (oracle.mg(L, r, coloured=True) == ref.mg_permuted(r)).all()
+        bb = oracle.spmv(L[0], u)
+        for coloured in (False, True):
+            f = ref.cg_permuted if coloured else ref.cg
+            got = f(bb, np.zeros(n), 10, 0.0)
+            ox, ok, onr, onr0 = oracle.cg(L, bb, np.zeros(n), 10, 0.0, coloured=coloured)
+            assert got[1] == ok
+            assert abs(got[3] / onr0 - 1) < 1e-13
+            # within 1e-8 of each other, or both at the round-off floor
+            assert abs(got[2] - onr) <= 1e-8 * onr + 1e-13 * onr0
+            assert np.abs(got[0] - ox).max() <= 1e-10 * np.abs(ox).max()
+    finally:
+        ref.close()
+
+
 def test_mixed_oracle_consistency(oracle):
     """The FP32/BF16 restatement reduces to exact BF16 values on the HPCG
     stencil (26 and -1 are BF16-exact) and its flexible CG converges."""
