@@ -114,3 +114,26 @@ def test_reference_arm_unavailable_line(monkeypatch, capsys):
     assert len(out) == 1
     rec = json.loads(out[0])
     assert rec["impl"] == "reference" and "unavailable" in rec
+
+
+def test_reference_iteration_table_against_the_reference():
+    """The measured entries of bench.REF_NATURAL_ITERS that run in seconds
+    (32^3, 64^3): CG_ref of the reference build on the bench's system
+    (b = A u, u ~ U(-1, 1) seed 1, x0 = 0) to 1e-10 takes that many
+    iterations.  The table scales the CPU baseline to the benchmark grid."""
+    import numpy as np
+    import pytest
+    import bench
+    from oracle.oracle import Oracle, RefProblem, build
+    build()
+    if not RefProblem.available():
+        pytest.skip("oracle/_ref not built (needs the reference sources)")
+    for n in (32, 64):
+        ref = RefProblem(n, n, n)
+        try:
+            u = Oracle.uniform(bench.SEED_U, ref.rows(0), -1.0, 1.0)
+            b = ref.spmv(0, u)
+            _, k, nr, nr0, _ = ref.cg(b, np.zeros(ref.rows(0)), 500, bench.TOL)
+        finally:
+            ref.close()
+        assert k == bench.REF_NATURAL_ITERS[n] and nr <= bench.TOL * nr0, (n, k)
