@@ -287,3 +287,28 @@ def test_matrix_free_restatements_match_stored(dims, oracle):
             assert (oracle.stencil_spmv(dims, u) == R.spmv(0, u)).all()
         finally:
             R.close()
+
+
+def test_bf16_rounding_against_torch(oracle):
+    """The FP64 -> BF16 conversion of the mixed V-cycle's values (through
+    FP32, nearest-even at each step) equals torch's float64 -> float32 ->
+    bfloat16 conversion: random magnitudes, exact ties in both parities,
+    FP32 subnormals, signed zeros and infinities; a NaN stays a NaN (its bit
+    pattern is each implementation's own)."""
+    rng = np.random.default_rng(7)
+    v = np.concatenate([
+        rng.standard_normal(20000) * 10.0 ** rng.integers(-40, 39, 20000),
+        -np.exp(0.5 * rng.standard_normal(5000)),               # variable-coefficient values
+        [0.0, -0.0, np.inf, -np.inf, np.nan, 26.0, -1.0, 1e-45, -1e-44, 3.4e38, 1e39],
+    ])
+    # FP32 values halfway between two BF16 values, with even and odd BF16 lsb
+    hi = rng.integers(0, 0x7f7f, 4000, dtype=np.uint32) << 16
+    ties = (hi | 0x8000).view(np.float32).astype(np.float64)
+    v = np.concatenate([v, ties, -ties])
+    import torch
+    lib = oracle.lib()
+    got = np.array([lib.or_bf16_from_double(float(x)) for x in v], dtype=np.uint16)
+    want = torch.from_numpy(v).to(torch.float32).to(torch.bfloat16).view(torch.int16).numpy()
+    nan = np.isnan(v)
+    assert (got[~nan] == want.view(np.uint16)[~nan]).all()
+    assert ((got[nan] & 0x7f80) == 0x7f80).all() and ((got[nan] & 0x7f) != 0).all()
