@@ -66,6 +66,16 @@ def seeded(oracle, n):
     return oracle.uniform(11, n, 1.0, 2.0), oracle.uniform(12, n), oracle.uniform(13, n)
 
 
+def test_device_uniform_draws_match_the_oracle(oracle):
+    """hpcgx_fill_uniform draws what Oracle.uniform draws (SplitMix64 counters,
+    lo + (hi - lo) u rounded one step at a time), so the bench's GPU solve and
+    its CPU baseline solve the same system b = A u."""
+    _, _, _, P = setup((16, 16, 16), oracle)
+    n = P.rows()
+    for seed, lo, hi in ((1, -1.0, 1.0), (12, 0.0, 1.0), (99, 1.0, 2.0)):
+        assert (host(P.fill_uniform(seed, lo, hi)) == oracle.uniform(seed, n, lo, hi)).all()
+
+
 def test_device_generator_matches_host_load(grid, oracle):
     _, _, _, P1 = setup(grid, oracle, "load")
     _, _, _, P2 = setup(grid, oracle, "generate")
